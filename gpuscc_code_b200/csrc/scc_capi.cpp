@@ -1,0 +1,721 @@
+// C ABI of the SCC engine: contexts, device residency, the whole-solve
+// launch and the phase-level entry points (see include/scc_capi.h).
+#include <cuda_runtime.h>
+
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <vector>
+
+#include "scc_capi.h"
+#include "scc_engine.h"
+#include "scc_internal.h"
+
+namespace sccb {
+
+static thread_local char g_err[1024] = "";
+
+int set_error(int code, const char *fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  std::vsnprintf(g_err, sizeof(g_err), fmt, ap);
+  va_end(ap);
+  return code;
+}
+void clear_error() { g_err[0] = 0; }
+
+}  // namespace sccb
+
+using sccb::set_error;
+
+namespace {
+
+struct DBuf {
+  void *p = nullptr;
+  size_t bytes = 0;
+  cudaError_t ensure(size_t b) {
+    if (b == 0) b = 16;
+    if (b <= bytes) return cudaSuccess;
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+    cudaError_t e = cudaMalloc(&p, b);
+    if (e == cudaSuccess) bytes = b;
+    return e;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+  }
+  template <class T>
+  T *as() const {
+    return reinterpret_cast<T *>(p);
+  }
+};
+
+}  // namespace
+
+struct scc_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  scc_opts opts{};
+  // bound graph
+  uint32_t n = 0, m = 0;
+  int sorted_unique = 0;
+  bool have_graph = false;
+  const uint32_t *d_off = nullptr, *d_adj = nullptr, *d_offT = nullptr, *d_adjT = nullptr;
+  DBuf g_off, g_adj, g_offT, g_adjT;  // owned graph storage
+  // per-vertex state
+  uint32_t cap_n = 0, cap_h = 0;
+  bool have_state = false;
+  DBuf label, range, rpivot, aux, bitmaps, qa, qb, act0, act1, piv, pivkey, slot, heavy, ctl, seg;
+  uint32_t nwords = 0;
+  bool slot_dirty = true;
+  uint32_t nseg = 0;
+  std::vector<uint32_t> seg_host;
+  bool phase_ready = false;
+  sccb::Ctl *h_ctl = nullptr;  // pinned
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  uint32_t grid_used = 0;
+  uint32_t launches = 0;
+  uint32_t *enq_labels = nullptr;
+};
+
+namespace {
+
+int cuda_fail(cudaError_t e, const char *what) {
+  return set_error(e == cudaErrorMemoryAllocation ? SCC_ERR_NOMEM : SCC_ERR_CUDA, "%s: %s", what,
+                   cudaGetErrorString(e));
+}
+#define CK(call, what)                          \
+  do {                                          \
+    cudaError_t e_ = (call);                    \
+    if (e_ != cudaSuccess) return cuda_fail(e_, what); \
+  } while (0)
+
+int use_device(scc_ctx *c) {
+  CK(cudaSetDevice(c->device), "cudaSetDevice");
+  return SCC_OK;
+}
+
+int check_opts(const scc_opts *o) {
+  if (o->alg < SCC_ALG_QUADRATIC || o->alg > SCC_ALG_BEST) return set_error(SCC_ERR_INVALID, "unknown alg %d", o->alg);
+  if (o->block_size != 0 && o->block_size != 128 && o->block_size != 256 && o->block_size != 512 &&
+      o->block_size != 1024)
+    return set_error(SCC_ERR_INVALID, "block_size must be 128, 256, 512 or 1024 (got %d)", o->block_size);
+  if (o->pivot_rule < 0 || o->pivot_rule > 1) return set_error(SCC_ERR_INVALID, "unknown pivot rule %d", o->pivot_rule);
+  if (o->switch_permille < 0 || o->switch_permille > 1000)
+    return set_error(SCC_ERR_INVALID, "switch_permille must be in 0..1000");
+  if (o->heavy_degree != 0 && o->heavy_degree < 256) return set_error(SCC_ERR_INVALID, "heavy_degree must be >= 256");
+  return SCC_OK;
+}
+
+int ensure_state(scc_ctx *c) {
+  const uint32_t n = c->n;
+  const uint32_t hcap = c->m / 256u + 2u;
+  if (c->have_state && n <= c->cap_n && hcap <= c->cap_h) return SCC_OK;
+  const uint32_t cn = n > c->cap_n ? n : c->cap_n;
+  const uint32_t ch = hcap > c->cap_h ? hcap : c->cap_h;
+  const size_t vb = ((size_t)cn + 1) * 4;
+  const uint32_t nw = ((((uint32_t)(((uint64_t)cn + 1 + 31) / 32)) + 3u) & ~3u) + 4u;
+  CK(c->label.ensure(vb), "alloc labels");
+  CK(c->range.ensure(vb), "alloc ranges");
+  CK(c->rpivot.ensure(vb), "alloc pivots");
+  CK(c->aux.ensure(vb), "alloc aux");
+  CK(c->bitmaps.ensure((size_t)nw * 4 * 7), "alloc bitmaps");
+  CK(c->qa.ensure(vb), "alloc queue");
+  CK(c->qb.ensure(vb), "alloc queue");
+  CK(c->act0.ensure(vb), "alloc active list");
+  CK(c->act1.ensure(vb), "alloc active list");
+  CK(c->piv.ensure(vb), "alloc pivot list");
+  CK(c->pivkey.ensure(vb), "alloc pivot keys");
+  const size_t slot_bytes = ((size_t)cn + 1) * 3 * 8;
+  if (slot_bytes > c->slot.bytes) c->slot_dirty = true;
+  CK(c->slot.ensure(slot_bytes), "alloc election slots");
+  CK(c->heavy.ensure((size_t)ch * 5 * 4), "alloc heavy list");
+  CK(c->ctl.ensure(sizeof(sccb::Ctl)), "alloc control block");
+  if (c->slot_dirty) {
+    CK(cudaMemsetAsync(c->slot.p, 0xff, c->slot.bytes, c->stream), "init election slots");
+    c->slot_dirty = false;
+  }
+  c->cap_n = cn;
+  c->cap_h = ch;
+  c->nwords = nw;
+  c->have_state = true;
+  return SCC_OK;
+}
+
+sccb::Params make_params(scc_ctx *c, uint32_t *out_labels) {
+  sccb::Params p{};
+  p.g.n = c->n;
+  p.g.m = c->m;
+  p.g.sorted_unique = c->sorted_unique ? 1u : 0u;
+  p.g.off = c->d_off;
+  p.g.adj = c->d_adj;
+  p.g.offT = c->d_offT;
+  p.g.adjT = c->d_adjT;
+  sccb::EngState &s = p.s;
+  s.label = c->label.as<uint32_t>();
+  s.range = c->range.as<uint32_t>();
+  s.rpivot = c->rpivot.as<uint32_t>();
+  s.aux = c->aux.as<uint32_t>();
+  // bitmaps sized for this graph (words beyond it are never touched)
+  const uint32_t nw = ((((uint32_t)(((uint64_t)c->n + 1 + 31) / 32)) + 3u) & ~3u);
+  uint32_t *bm = c->bitmaps.as<uint32_t>();
+  const uint32_t stride = c->nwords;
+  s.elim = bm + 0 * (size_t)stride;
+  s.fvis = bm + 1 * (size_t)stride;
+  s.bvis = bm + 2 * (size_t)stride;
+  s.fexp = bm + 3 * (size_t)stride;
+  s.bexp = bm + 4 * (size_t)stride;
+  s.tflag = bm + 5 * (size_t)stride;
+  s.queued = bm + 6 * (size_t)stride;
+  s.qa = c->qa.as<uint32_t>();
+  s.qb = c->qb.as<uint32_t>();
+  s.act[0] = c->act0.as<uint32_t>();
+  s.act[1] = c->act1.as<uint32_t>();
+  s.piv = c->piv.as<uint32_t>();
+  s.pivkey = c->pivkey.as<uint32_t>();
+  s.slot = c->slot.as<unsigned long long>();
+  uint32_t *h = c->heavy.as<uint32_t>();
+  s.hv = h;
+  s.hbeg = h + (size_t)c->cap_h;
+  s.hdeg = h + 2 * (size_t)c->cap_h;
+  s.htag = h + 3 * (size_t)c->cap_h;
+  s.hbase = h + 4 * (size_t)c->cap_h;
+  s.seg = c->nseg > 1 ? c->seg.as<uint32_t>() : nullptr;
+  s.out_labels = out_labels;
+  s.ctl = c->ctl.as<sccb::Ctl>();
+  s.nwords = nw;
+  s.qcap = c->n + 1;
+  s.hcap = c->cap_h;
+  s.nseg = c->nseg > 1 ? c->nseg : 1;
+  const scc_opts &o = c->opts;
+  sccb::EngOpts &e = p.o;
+  e.alg = (uint32_t)o.alg;
+  e.wcc = o.wcc ? 1u : 0u;
+  e.trim2 = o.trim2 ? 1u : 0u;
+  e.trim_first = o.trim_first ? 1u : 0u;
+  e.pivot_rule = (uint32_t)o.pivot_rule;
+  e.switch_thr = (uint32_t)((uint64_t)c->n * (uint64_t)o.switch_permille / 1000ull);
+  e.trim_depth = o.trim_depth;
+  e.pull_alpha = o.pull_alpha;
+  e.pull_beta = o.pull_beta;
+  e.warp_degree = o.warp_degree ? o.warp_degree : 32u;
+  e.heavy_degree = o.heavy_degree ? o.heavy_degree : 4096u;
+  e.max_iters = o.max_iters ? o.max_iters : (1u << 20);
+  e.timeout_ns = (unsigned long long)(o.timeout_ms ? o.timeout_ms : 10000u) * 1000000ull;
+  return p;
+}
+
+int block_size_of(const scc_ctx *c) { return c->opts.block_size ? c->opts.block_size : 256; }
+
+int need_graph(scc_ctx *c) {
+  if (!c) return set_error(SCC_ERR_INVALID, "null context");
+  if (!c->have_graph) return set_error(SCC_ERR_STATE, "no graph bound to the context");
+  if (c->nseg > 1 && c->seg_host.back() != c->n + 1)
+    return set_error(SCC_ERR_INVALID, "segments end at %u but the graph has %u vertices", c->seg_host.back() - 1, c->n);
+  if (c->nseg > 1 && c->nseg > c->n)
+    return set_error(SCC_ERR_INVALID, "%u segments for %u vertices (partition ids must stay below n+1)", c->nseg, c->n);
+  return SCC_OK;
+}
+
+int read_ctl(scc_ctx *c) {
+  CK(cudaMemcpyAsync(c->h_ctl, c->ctl.p, sizeof(sccb::Ctl), cudaMemcpyDeviceToHost, c->stream), "read control block");
+  CK(cudaStreamSynchronize(c->stream), "synchronise");
+  if (c->h_ctl->gs.err) {
+    c->slot_dirty = true;
+    c->phase_ready = false;
+    const uint32_t e = c->h_ctl->gs.err;
+    return set_error(SCC_ERR_TIMEOUT, "device-side %s (flags 0x%x, at barrier %u)",
+                     (e & 1u) ? "barrier wait timed out" : (e & 2u) ? "iteration cap reached" : "queue overflow", e,
+                     c->h_ctl->gs.err_where);
+  }
+  return SCC_OK;
+}
+
+int launch(scc_ctx *c, uint32_t phase, uint32_t a0 = 0, uint32_t a1 = 0, uint32_t a2 = 0,
+           uint32_t *out_labels = nullptr) {
+  const sccb::Params p = make_params(c, out_labels);
+  CK(sccb::launch_phase(p, phase, a0, a1, a2, block_size_of(c), c->opts.grid_blocks, c->stream, &c->grid_used),
+     "cooperative launch");
+  ++c->launches;
+  return SCC_OK;
+}
+
+int reset_state(scc_ctx *c) {
+  int rc = ensure_state(c);
+  if (rc) return rc;
+  CK(cudaMemsetAsync(c->ctl.p, 0, sizeof(sccb::Ctl), c->stream), "clear control block");
+  const sccb::Params p = make_params(c, nullptr);
+  CK(sccb::launch_init(p, c->stream), "init launch");
+  ++c->launches;
+  return SCC_OK;
+}
+
+void fill_stats(scc_ctx *c, scc_stats *st, float ms) {
+  if (!st) return;
+  const sccb::Ctl &k = *c->h_ctl;
+  std::memset(st, 0, sizeof(*st));
+  st->steps = k.steps;
+  st->fwd_depth = k.fwd_depth;
+  st->bwd_depth = k.bwd_depth;
+  st->trim_iters = k.trim_iters;
+  st->wcc_iters = k.wcc_iters;
+  st->wcc_step = k.wcc_step;
+  st->n_trimmed = k.n_trimmed;
+  st->n_trim2 = k.n_trim2;
+  st->n_fb_elim = k.n_fbe + k.n_trim2;
+  st->nscc = k.nscc;
+  st->pull_sweeps = k.pull_sweeps;
+  st->grid_blocks = c->grid_used;
+  st->block_size = (uint32_t)block_size_of(c);
+  st->kernel_launches = c->launches;
+  st->ms_total = ms;
+  st->ms_trim = k.ns_trim * 1e-6;
+  st->ms_fwd = k.ns_fwd * 1e-6;
+  st->ms_bwd = k.ns_bwd * 1e-6;
+  st->ms_update = k.ns_update * 1e-6;
+  st->ms_wcc = k.ns_wcc * 1e-6;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *scc_last_error(void) { return sccb::g_err; }
+const char *scc_version(void) { return "gpuscc_b200 1.0 (sm_100a)"; }
+
+void scc_opts_default(scc_opts *o) {
+  if (!o) return;
+  std::memset(o, 0, sizeof(*o));
+  o->alg = SCC_ALG_TOPO;  // scc.cu:80
+  o->wcc = 0;
+  o->trim2 = 0;
+  o->trim_first = 1;  // scc.cu:38 TRIM_FIRST
+  o->block_size = 256;  // scc.cu:82
+  o->warp_size = 32;  // scc.cu:81
+  o->pivot_rule = SCC_PIVOT_MIN_ID;
+  o->switch_permille = 10;  // n/100 (scc.cu:507)
+  o->trim_depth = 0;
+  o->pull_alpha = 0;
+  o->pull_beta = 0;
+}
+
+int scc_ctx_create(int device, const scc_opts *opts, scc_ctx **out) {
+  sccb::clear_error();
+  if (!out) return set_error(SCC_ERR_INVALID, "null output");
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return set_error(SCC_ERR_NODEVICE, "no CUDA device available");
+  }
+  if (device < 0 || device >= ndev) return set_error(SCC_ERR_INVALID, "device %d out of range (have %d)", device, ndev);
+  scc_opts o;
+  scc_opts_default(&o);
+  if (opts) o = *opts;
+  int rc = check_opts(&o);
+  if (rc) return rc;
+  scc_ctx *c = new scc_ctx();
+  c->device = device;
+  c->opts = o;
+  cudaError_t e = cudaSetDevice(device);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaMallocHost((void **)&c->h_ctl, sizeof(sccb::Ctl));
+  if (e == cudaSuccess) e = cudaEventCreate(&c->ev0);
+  if (e == cudaSuccess) e = cudaEventCreate(&c->ev1);
+  if (e != cudaSuccess) {
+    scc_ctx_destroy(c);
+    return cuda_fail(e, "context setup");
+  }
+  *out = c;
+  return SCC_OK;
+}
+
+int scc_ctx_destroy(scc_ctx *c) {
+  if (!c) return SCC_OK;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  for (DBuf *b : {&c->g_off, &c->g_adj, &c->g_offT, &c->g_adjT, &c->label, &c->range, &c->rpivot, &c->aux,
+                  &c->bitmaps, &c->qa, &c->qb, &c->act0, &c->act1, &c->piv, &c->pivkey, &c->slot, &c->heavy,
+                  &c->ctl, &c->seg})
+    b->release();
+  if (c->h_ctl) cudaFreeHost(c->h_ctl);
+  if (c->ev0) cudaEventDestroy(c->ev0);
+  if (c->ev1) cudaEventDestroy(c->ev1);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+  return SCC_OK;
+}
+
+int scc_ctx_set_opts(scc_ctx *c, const scc_opts *o) {
+  sccb::clear_error();
+  if (!c || !o) return set_error(SCC_ERR_INVALID, "null argument");
+  int rc = check_opts(o);
+  if (rc) return rc;
+  c->opts = *o;
+  return SCC_OK;
+}
+
+int scc_ctx_get_opts(const scc_ctx *c, scc_opts *o) {
+  if (!c || !o) return set_error(SCC_ERR_INVALID, "null argument");
+  *o = c->opts;
+  return SCC_OK;
+}
+
+void *scc_ctx_stream(scc_ctx *c) { return c ? (void *)c->stream : nullptr; }
+
+int scc_ctx_upload(scc_ctx *c, const scc_host_csr *g) {
+  sccb::clear_error();
+  if (!c || !g) return set_error(SCC_ERR_INVALID, "null argument");
+  if (g->n >= (1u << 30)) return set_error(SCC_ERR_CAPACITY, "n must be below 2^30");
+  if (!g->nodes || !g->nodesT || (g->m && (!g->edges || !g->edgesT))) return set_error(SCC_ERR_INVALID, "null arrays");
+  if (g->nodes[g->n + 1] != g->m || g->nodesT[g->n + 1] != g->m)
+    return set_error(SCC_ERR_INVALID, "nodes[n+1] (%u) / nodesT[n+1] (%u) differ from m (%u)", g->nodes[g->n + 1],
+                     g->nodesT[g->n + 1], g->m);
+  // the kernels trust the layout: reject anything that would index outside it
+  for (int t = 0; t < 2; ++t) {
+    const uint32_t *o = t ? g->nodesT : g->nodes, *a = t ? g->edgesT : g->edges;
+    if (g->n && o[1] != 0) return set_error(SCC_ERR_INVALID, "%s[1] must be 0", t ? "nodesT" : "nodes");
+    for (uint32_t v = 1; v <= g->n; ++v)
+      if (o[v] > o[v + 1]) return set_error(SCC_ERR_INVALID, "%s decreases at vertex %u", t ? "nodesT" : "nodes", v);
+    for (uint32_t i = 0; i < g->m; ++i)
+      if (a[i] < 1 || a[i] > g->n)
+        return set_error(SCC_ERR_INVALID, "%s[%u] = %u is outside 1..%u", t ? "edgesT" : "edges", i, a[i], g->n);
+  }
+  int rc = use_device(c);
+  if (rc) return rc;
+  const size_t ob = ((size_t)g->n + 2) * 4, eb = ((size_t)g->m + 1) * 4;
+  CK(c->g_off.ensure(ob), "alloc graph");
+  CK(c->g_adj.ensure(eb), "alloc graph");
+  CK(cudaMemcpyAsync(c->g_off.p, g->nodes, ob, cudaMemcpyHostToDevice, c->stream), "upload nodes");
+  if (g->m) CK(cudaMemcpyAsync(c->g_adj.p, g->edges, (size_t)g->m * 4, cudaMemcpyHostToDevice, c->stream), "upload edges");
+  c->d_off = c->g_off.as<uint32_t>();
+  c->d_adj = c->g_adj.as<uint32_t>();
+  if (g->nodesT == g->nodes && g->edgesT == g->edges) {
+    c->d_offT = c->d_off;
+    c->d_adjT = c->d_adj;
+  } else {
+    CK(c->g_offT.ensure(ob), "alloc graph");
+    CK(c->g_adjT.ensure(eb), "alloc graph");
+    CK(cudaMemcpyAsync(c->g_offT.p, g->nodesT, ob, cudaMemcpyHostToDevice, c->stream), "upload nodesT");
+    if (g->m)
+      CK(cudaMemcpyAsync(c->g_adjT.p, g->edgesT, (size_t)g->m * 4, cudaMemcpyHostToDevice, c->stream), "upload edgesT");
+    c->d_offT = c->g_offT.as<uint32_t>();
+    c->d_adjT = c->g_adjT.as<uint32_t>();
+  }
+  c->n = g->n;
+  c->m = g->m;
+  c->sorted_unique = g->sorted_unique;
+  c->have_graph = true;
+  c->phase_ready = false;
+  CK(cudaStreamSynchronize(c->stream), "upload");
+  return ensure_state(c);
+}
+
+int scc_gen_rmat_device(scc_ctx *c, uint32_t scale, uint64_t samples, uint32_t a_ppm, uint32_t b_ppm,
+                        uint32_t c_ppm, uint64_t seed, int permute, scc_dev_csr *out) {
+  sccb::clear_error();
+  if (!c) return set_error(SCC_ERR_INVALID, "null context");
+  if (scale < 1 || scale > 29 || samples >= (1ull << 31) || (uint64_t)a_ppm + b_ppm + c_ppm > 1000000ull)
+    return set_error(SCC_ERR_INVALID, "bad R-MAT arguments");
+  int rc = use_device(c);
+  if (rc) return rc;
+  for (DBuf *b : {&c->g_off, &c->g_adj, &c->g_offT, &c->g_adjT}) b->release();
+  c->have_graph = false;
+  uint32_t *off = nullptr, *adj = nullptr, *offT = nullptr, *adjT = nullptr, m = 0;
+  CK(sccb::gen_rmat_device(scale, samples, a_ppm, b_ppm, c_ppm, seed, permute, c->stream, &off, &adj, &offT, &adjT, &m),
+     "device R-MAT build");
+  const uint32_t n = 1u << scale;
+  c->g_off.p = off;
+  c->g_off.bytes = ((size_t)n + 2) * 4;
+  c->g_adj.p = adj;
+  c->g_adj.bytes = ((size_t)m + 1) * 4;
+  c->g_offT.p = offT;
+  c->g_offT.bytes = ((size_t)n + 2) * 4;
+  c->g_adjT.p = adjT;
+  c->g_adjT.bytes = ((size_t)m + 1) * 4;
+  c->d_off = off;
+  c->d_adj = adj;
+  c->d_offT = offT;
+  c->d_adjT = adjT;
+  c->n = n;
+  c->m = m;
+  c->sorted_unique = 1;
+  c->have_graph = true;
+  c->phase_ready = false;
+  if (out) {
+    out->n = n;
+    out->m = m;
+    out->sorted_unique = 1;
+    out->nodes = off;
+    out->edges = adj;
+    out->nodesT = offT;
+    out->edgesT = adjT;
+  }
+  return ensure_state(c);
+}
+
+int scc_ctx_bind_device(scc_ctx *c, const scc_dev_csr *g) {
+  sccb::clear_error();
+  if (!c || !g) return set_error(SCC_ERR_INVALID, "null argument");
+  if (g->n >= (1u << 30)) return set_error(SCC_ERR_CAPACITY, "n must be below 2^30");
+  if (!g->nodes || !g->nodesT || (g->m && (!g->edges || !g->edgesT))) return set_error(SCC_ERR_INVALID, "null arrays");
+  int rc = use_device(c);
+  if (rc) return rc;
+  CK(c->ctl.ensure(sizeof(sccb::Ctl)), "alloc control block");
+  if (!c->h_ctl) return set_error(SCC_ERR_STATE, "context not initialised");
+  for (int t = 0; t < 2; ++t) {
+    uint32_t bad = 0;
+    CK(sccb::check_device_csr(t ? g->nodesT : g->nodes, t ? g->edgesT : g->edges, g->n, g->m, c->ctl.as<uint32_t>(),
+                              &bad, c->stream),
+       "device CSR check");
+    if (bad)
+      return set_error(SCC_ERR_INVALID, "device %s: %s", t ? "transpose" : "graph",
+                       (bad & 1u) ? "offsets are not monotone from 0 to m" : "a neighbour id is outside 1..n");
+  }
+  c->d_off = g->nodes;
+  c->d_adj = g->edges;
+  c->d_offT = g->nodesT;
+  c->d_adjT = g->edgesT;
+  c->n = g->n;
+  c->m = g->m;
+  c->sorted_unique = g->sorted_unique;
+  c->have_graph = true;
+  c->phase_ready = false;
+  return ensure_state(c);
+}
+
+int scc_ctx_download(scc_ctx *c, scc_host_csr *out) {
+  sccb::clear_error();
+  int rc = need_graph(c);
+  if (rc) return rc;
+  if (!out) return set_error(SCC_ERR_INVALID, "null output");
+  rc = use_device(c);
+  if (rc) return rc;
+  std::memset(out, 0, sizeof(*out));
+  const size_t ob = ((size_t)c->n + 2) * 4, eb = ((size_t)c->m + 1) * 4;
+  out->nodes = (uint32_t *)std::malloc(ob);
+  out->edges = (uint32_t *)std::malloc(eb);
+  out->nodesT = (uint32_t *)std::malloc(ob);
+  out->edgesT = (uint32_t *)std::malloc(eb);
+  out->owned = 1;
+  if (!out->nodes || !out->edges || !out->nodesT || !out->edgesT) {
+    scc_host_csr_free(out);
+    return set_error(SCC_ERR_NOMEM, "host allocation failed");
+  }
+  CK(cudaMemcpy(out->nodes, c->d_off, ob, cudaMemcpyDeviceToHost), "download");
+  CK(cudaMemcpy(out->nodesT, c->d_offT, ob, cudaMemcpyDeviceToHost), "download");
+  if (c->m) {
+    CK(cudaMemcpy(out->edges, c->d_adj, (size_t)c->m * 4, cudaMemcpyDeviceToHost), "download");
+    CK(cudaMemcpy(out->edgesT, c->d_adjT, (size_t)c->m * 4, cudaMemcpyDeviceToHost), "download");
+  }
+  out->edges[c->m] = 0;
+  out->edgesT[c->m] = 0;
+  out->nodes[0] = 0;
+  out->nodesT[0] = 0;
+  out->n = c->n;
+  out->m = c->m;
+  out->nnz_header = c->m;
+  out->sorted_unique = c->sorted_unique;
+  return SCC_OK;
+}
+
+int scc_ctx_set_segments(scc_ctx *c, uint32_t nseg, const uint32_t *seg_first) {
+  sccb::clear_error();
+  if (!c) return set_error(SCC_ERR_INVALID, "null context");
+  if (nseg == 0) {
+    c->nseg = 0;
+    c->seg_host.clear();
+    return SCC_OK;
+  }
+  if (!seg_first) return set_error(SCC_ERR_INVALID, "null segment table");
+  if (seg_first[0] != 1) return set_error(SCC_ERR_INVALID, "seg_first[0] must be 1");
+  for (uint32_t s = 0; s < nseg; ++s)
+    if (seg_first[s + 1] < seg_first[s]) return set_error(SCC_ERR_INVALID, "segment table not monotone at %u", s);
+  int rc = use_device(c);
+  if (rc) return rc;
+  c->seg_host.assign(seg_first, seg_first + nseg + 1);
+  CK(c->seg.ensure(((size_t)nseg + 1) * 4), "alloc segments");
+  CK(cudaMemcpy(c->seg.p, seg_first, ((size_t)nseg + 1) * 4, cudaMemcpyHostToDevice), "upload segments");
+  c->nseg = nseg;
+  c->phase_ready = false;
+  return SCC_OK;
+}
+
+int scc_solve_enqueue(scc_ctx *c, uint32_t *d_labels) {
+  sccb::clear_error();
+  int rc = need_graph(c);
+  if (rc) return rc;
+  rc = use_device(c);
+  if (rc) return rc;
+  c->launches = 0;
+  rc = reset_state(c);
+  if (rc) return rc;
+  CK(cudaEventRecord(c->ev0, c->stream), "event");
+  rc = launch(c, sccb::PH_SOLVE, 0, 0, 0, d_labels);
+  if (rc) return rc;
+  CK(cudaEventRecord(c->ev1, c->stream), "event");
+  c->enq_labels = d_labels;
+  c->phase_ready = false;
+  return SCC_OK;
+}
+
+int scc_solve_collect(scc_ctx *c, uint32_t *nscc, scc_stats *st) {
+  if (!c) return set_error(SCC_ERR_INVALID, "null context");
+  int rc = read_ctl(c);
+  if (rc) return rc;
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+  if (c->h_ctl->phase_ret != 0)
+    return set_error(SCC_ERR_STATE, "%u vertices left without a component", c->h_ctl->phase_ret);
+  if (nscc) *nscc = c->h_ctl->nscc;
+  fill_stats(c, st, ms);
+  return SCC_OK;
+}
+
+int scc_solve_device(scc_ctx *c, uint32_t *d_labels, uint32_t *nscc, scc_stats *st) {
+  int rc = scc_solve_enqueue(c, d_labels);
+  if (rc) return rc;
+  return scc_solve_collect(c, nscc, st);
+}
+
+int scc_solve(scc_ctx *c, uint32_t *labels, uint32_t *nscc, scc_stats *st) {
+  int rc = scc_solve_device(c, nullptr, nscc, st);
+  if (rc) return rc;
+  if (labels) {
+    CK(cudaMemcpyAsync(labels, c->label.p, ((size_t)c->n + 1) * 4, cudaMemcpyDeviceToHost, c->stream), "labels D2H");
+    CK(cudaStreamSynchronize(c->stream), "labels D2H");
+    labels[0] = 0;
+  }
+  return SCC_OK;
+}
+
+// ------------------------------------------------------------- phases
+static int phase_prologue(scc_ctx *c) {
+  sccb::clear_error();
+  int rc = need_graph(c);
+  if (rc) return rc;
+  rc = use_device(c);
+  if (rc) return rc;
+  if (!c->phase_ready) return set_error(SCC_ERR_STATE, "call scc_phase_begin first");
+  return SCC_OK;
+}
+
+static int run_phase(scc_ctx *c, uint32_t phase, uint32_t a0 = 0, uint32_t a1 = 0, uint32_t a2 = 0) {
+  int rc = phase_prologue(c);
+  if (rc) return rc;
+  rc = launch(c, phase, a0, a1, a2);
+  if (rc) return rc;
+  return read_ctl(c);
+}
+
+int scc_phase_begin(scc_ctx *c) {
+  sccb::clear_error();
+  int rc = need_graph(c);
+  if (rc) return rc;
+  rc = use_device(c);
+  if (rc) return rc;
+  rc = reset_state(c);
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(c->stream), "phase begin");
+  c->phase_ready = true;
+  return SCC_OK;
+}
+
+int scc_trim1(scc_ctx *c, uint32_t *it) {
+  int rc = run_phase(c, sccb::PH_TRIM1);
+  if (!rc && it) *it = c->h_ctl->phase_ret;
+  return rc;
+}
+int scc_trim(scc_ctx *c, uint32_t *it) {
+  int rc = run_phase(c, sccb::PH_TRIM);
+  if (!rc && it) *it = c->h_ctl->phase_ret;
+  return rc;
+}
+int scc_trim2(scc_ctx *c, uint32_t *removed) {
+  int rc = run_phase(c, sccb::PH_TRIM2);
+  if (!rc && removed) *removed = c->h_ctl->phase_ret;
+  return rc;
+}
+int scc_select_pivots(scc_ctx *c, uint32_t *np) {
+  int rc = run_phase(c, sccb::PH_SELECT);
+  if (!rc && np) *np = c->h_ctl->piv_count;
+  return rc;
+}
+int scc_reach(scc_ctx *c, int dir, int variant, int first_step, uint32_t *depth) {
+  if (dir != 0 && dir != 1) return set_error(SCC_ERR_INVALID, "dir must be 0 (forward) or 1 (backward)");
+  if (variant != SCC_ALG_QUADRATIC && variant != SCC_ALG_TOPO && variant != SCC_ALG_DATA &&
+      variant != SCC_ALG_LINEAR && variant != SCC_ALG_BEST)
+    return set_error(SCC_ERR_INVALID, "reach variant must be q, t, d, l or b");
+  int rc = run_phase(c, sccb::PH_REACH, (uint32_t)dir, (uint32_t)variant, first_step ? 0u : 1u);
+  if (!rc && depth) *depth = c->h_ctl->phase_ret;
+  return rc;
+}
+int scc_update(scc_ctx *c, int32_t *has_pivot) {
+  int rc = run_phase(c, sccb::PH_UPDATE);
+  if (!rc && has_pivot) *has_pivot = c->h_ctl->piv_count > 0;
+  return rc;
+}
+int scc_count_elimmed(scc_ctx *c, uint32_t *ne) {
+  int rc = phase_prologue(c);
+  if (rc) return rc;
+  rc = read_ctl(c);
+  if (!rc && ne) *ne = c->h_ctl->n_fbe + c->h_ctl->n_trim2;
+  return rc;
+}
+int scc_unset_pivots(scc_ctx *c) { return run_phase(c, sccb::PH_UNSET); }
+int scc_update_wcc(scc_ctx *c, uint32_t *depth, int32_t *has_pivot) {
+  int rc = run_phase(c, sccb::PH_WCC);
+  if (!rc) {
+    if (depth) *depth = c->h_ctl->phase_ret;
+    if (has_pivot) *has_pivot = c->h_ctl->piv_count > 0;
+  }
+  return rc;
+}
+int scc_get_states(scc_ctx *c, uint8_t *states) {
+  int rc = phase_prologue(c);
+  if (rc) return rc;
+  if (!states) return set_error(SCC_ERR_INVALID, "null output");
+  void *d = nullptr;
+  CK(cudaMalloc(&d, (size_t)c->n + 1), "alloc");
+  const sccb::Params p = make_params(c, nullptr);
+  cudaError_t e = sccb::launch_states(p, (uint8_t *)d, c->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(states, d, (size_t)c->n + 1, cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  cudaFree(d);
+  if (e != cudaSuccess) return cuda_fail(e, "states export");
+  return SCC_OK;
+}
+int scc_get_ranges(scc_ctx *c, uint32_t *ranges) {
+  int rc = phase_prologue(c);
+  if (rc) return rc;
+  if (!ranges) return set_error(SCC_ERR_INVALID, "null output");
+  void *d = nullptr;
+  CK(cudaMalloc(&d, ((size_t)c->n + 1) * 4), "alloc");
+  const sccb::Params p = make_params(c, nullptr);
+  cudaError_t e = sccb::launch_ranges(p, (uint32_t *)d, c->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(ranges, d, ((size_t)c->n + 1) * 4, cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  cudaFree(d);
+  if (e != cudaSuccess) return cuda_fail(e, "ranges export");
+  return SCC_OK;
+}
+int scc_get_labels(scc_ctx *c, uint32_t *labels, uint32_t *nscc) {
+  int rc = run_phase(c, sccb::PH_FINALIZE);
+  if (rc) return rc;
+  if (c->h_ctl->phase_ret != 0)
+    return set_error(SCC_ERR_STATE, "%u vertices are not assigned to a component yet", c->h_ctl->phase_ret);
+  if (nscc) *nscc = c->h_ctl->nscc;
+  if (labels) {
+    CK(cudaMemcpy(labels, c->label.p, ((size_t)c->n + 1) * 4, cudaMemcpyDeviceToHost), "labels D2H");
+    labels[0] = 0;
+  }
+  return SCC_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,1191 @@
+// Persistent Forward-Backward SCC engine for B200 (sm_100a).
+//
+// One cooperative launch runs the whole reference driver loop
+// (scc.cu:217-910: trim-1, pivot, forward/backward reach, trim, update,
+// WCC + trim-2 once, repeat) with grid barriers instead of host round trips.
+// Each phase is a __device__ member of Eng; the phase-level C ABI launches
+// the same code one phase at a time.
+//
+// Per-vertex state (reference scc.h:48-93 packs it in one byte; here it is
+// split so the hot tests hit L2-resident bitmaps, n/8 bytes each):
+//   elim   - vertex already assigned to an SCC (reference bit E = 4)
+//   fvis   - forward visited (F = 2)          bvis - backward visited (B = 1)
+//   fexp   - forward expanded (FExt = 64)      bexp - backward expanded (BExt = 32)
+//   tflag  - removed by trim-1 (T = 8)         queued - trim candidate / trim-2 mark
+//   label  - u32 SCC label, range - u32 partition id (reference `ranges`).
+// Partition ids are exact: a refined partition is identified by the id of its
+// pivot, elected as the smallest (priority, id) key among its members, so the
+// reference's 3r+k hashing into 2^20 slots (scc_routines.cu:168-176) and its
+// collisions and wrap-around do not exist here.
+#include <cstdio>
+
+#include "scc_device.cuh"
+#include "scc_engine.h"
+
+namespace sccb {
+
+enum : uint32_t { C_CHG = 0, C_DEG = 1, C_Q = 2, C_Q2 = 3, C_CNT = 4, C_CNT2 = 5 };
+enum : uint32_t { ARM_Q = 0, ARM_T = 1, ARM_D = 2, ARM_L = 3, ARM_B = 6 };
+
+constexpr int kSlotCache = 128;  // per-CTA cache of partition-election slots
+
+template <int BS>
+struct Eng {
+  const Params &P;
+  Ctl *c;
+  uint32_t k;  // barrier interval index, identical in every CTA
+  uint32_t list_mode, act_count, act_sel;
+
+  __device__ explicit Eng(const Params &p) : P(p), c(p.s.ctl), k(0), list_mode(0), act_count(0), act_sel(0) {}
+
+  // ------------------------------------------------------------ plumbing
+  __device__ uint32_t *cur() { return c->ctr[k % 3]; }
+  __device__ uint32_t *prv() { return c->ctr[(k + 2) % 3]; }
+  __device__ unsigned long long *cur64() { return &c->ctr64[k % 3]; }
+  __device__ unsigned long long *prv64() { return &c->ctr64[(k + 2) % 3]; }
+  __device__ uint32_t rdprv(uint32_t i) { return ldm(prv() + i); }
+
+  __device__ bool bar(uint32_t where) {
+    if (blockIdx.x == 0) {
+      if (threadIdx.x < 16) c->ctr[(k + 1) % 3][threadIdx.x] = 0;
+      if (threadIdx.x == 16) c->ctr64[(k + 1) % 3] = 0;
+    }
+    const bool ok = grid_barrier(reinterpret_cast<GridSync *>(&c->gs), P.o.timeout_ns, where);
+    ++k;
+    return ok;
+  }
+  __device__ void refresh_mode() {
+    list_mode = ldm(&c->list_mode);
+    act_count = ldm(&c->act_count);
+    act_sel = ldm(&c->act_sel);
+  }
+  __device__ uint32_t *err() { return &c->gs.err; }
+  __device__ void fail(uint32_t bits) { atomicOr(&c->gs.err, bits); }
+  __device__ bool is_lead() { return blockIdx.x == 0 && threadIdx.x == 0; }
+
+  // block-reduced atomicAdd into a global counter
+  __device__ void add_count(uint32_t *dst, uint32_t x) {
+    const uint32_t s = block_sum(x);
+    if (threadIdx.x == 0 && s) atomicAdd(dst, s);
+  }
+
+  __device__ uint32_t gtid() const { return blockIdx.x * BS + threadIdx.x; }
+  __device__ uint32_t gstride() const { return gridDim.x * BS; }
+  __device__ uint32_t gwarp() const { return (blockIdx.x * BS + threadIdx.x) >> 5; }
+  __device__ uint32_t nwarps() const { return (gridDim.x * BS) >> 5; }
+
+  // Calls f(v, valid) for every vertex of the current sweep set, all 32
+  // lanes of a warp together (valid = false pads the last warp).  Full mode
+  // covers ids 0 .. nwords*32-1 so that a warp owns exactly one bitmap word.
+  template <class F>
+  __device__ void for_vertices(F &&f) {
+    if (list_mode) {
+      const uint32_t *lst = P.s.act[act_sel];
+      const uint32_t cnt = act_count;
+      const uint32_t lim = (cnt + 31u) & ~31u;
+      for (uint32_t i = gtid(); i < lim; i += gstride()) {
+        const bool valid = i < cnt;
+        f(valid ? ldm(lst + i) : 0u, valid);
+      }
+    } else {
+      const uint32_t lim = P.s.nwords * 32u;
+      const uint32_t n = P.g.n;
+      for (uint32_t v = gtid(); v < lim; v += gstride()) f(v, v >= 1 && v <= n);
+    }
+  }
+  // every id 0 .. nwords*32-1 regardless of the active list
+  template <class F>
+  __device__ void for_all_ids(F &&f) {
+    const uint32_t lim = P.s.nwords * 32u;
+    const uint32_t n = P.g.n;
+    for (uint32_t v = gtid(); v < lim; v += gstride()) f(v, v >= 1 && v <= n);
+  }
+  // grid-stride over [0, cnt), whole warps
+  template <class F>
+  __device__ void for_items(uint32_t cnt, F &&f) {
+    const uint32_t lim = (cnt + 31u) & ~31u;
+    for (uint32_t i = gtid(); i < lim; i += gstride()) f(i, i < cnt);
+  }
+
+  __device__ bool live(uint32_t v) const { return !bit_test(P.s.elim, v); }
+
+  __device__ uint32_t prio(uint32_t v) const {
+    if (P.o.pivot_rule == 0) return 0u;
+    const unsigned long long dout = ldg(P.g.off + v + 1) - ldg(P.g.off + v);
+    const unsigned long long din = ldg(P.g.offT + v + 1) - ldg(P.g.offT + v);
+    unsigned long long s = dout * din;
+    if (s > 0xfffffffeull) s = 0xfffffffeull;
+    return 0xfffffffeu - (uint32_t)s;
+  }
+
+  // ====================================================== trim-1 (a5/a6)
+  // scc_routines.cu:276-394: v is trimmed when it has no out-neighbour or no
+  // in-neighbour that is not itself, not eliminated and (ranged) in its
+  // partition.  Trimmed vertices become singleton SCCs (state 28).
+  __device__ bool live_nbr(const uint32_t *__restrict__ off, const uint32_t *__restrict__ adj, uint32_t v,
+                           uint32_t rv, bool ranged, bool snap) {
+    const uint32_t b = ldg(off + v), e = ldg(off + v + 1);
+    if (snap) {  // nothing eliminated yet and lists sorted-unique
+      const uint32_t d = e - b;
+      return d >= 2 || (d == 1 && ldg(adj + b) != v);
+    }
+    for (uint32_t i = b; i < e; ++i) {
+      const uint32_t u = ldg(adj + i);
+      if (u == v || !live(u)) continue;
+      if (ranged && ldm(P.s.range + u) != rv) continue;
+      return true;
+    }
+    return false;
+  }
+
+  __device__ void mark_trimmed(uint32_t v) {
+    P.s.label[v] = v;
+    bit_set(P.s.tflag, v);
+    bit_set(P.s.elim, v);
+  }
+
+  // Returns the number of trim iterations.  Iteration 1 sweeps the active
+  // set; later iterations only re-check neighbours of vertices trimmed in the
+  // previous one (deduplicated through the `queued` bitmap).
+  __device__ uint32_t trim(bool ranged, bool snap, uint32_t max_it) {
+    const EngState &s = P.s;
+    const EngGraph &g = P.g;
+    uint32_t ntrim = 0;
+    for_vertices([&](uint32_t v, bool valid) {
+      bool t = false;
+      if (valid && live(v)) {
+        const uint32_t rv = ranged ? ldm(s.range + v) : 0u;
+        t = !live_nbr(g.off, g.adj, v, rv, ranged, snap) || !live_nbr(g.offT, g.adjT, v, rv, ranged, snap);
+        if (t) mark_trimmed(v);
+      }
+      warp_push(s.qa, cur() + C_Q, s.qcap, v, t, err());
+      ntrim += t;
+    });
+    add_count(&c->n_trimmed, ntrim);
+    if (!bar(100)) return 1;
+    uint32_t it = 1;
+    uint32_t nq = rdprv(C_Q);
+    while (nq > 0 && it < max_it) {
+      // candidates: live partition-mates adjacent (either direction) to a vertex just trimmed
+      for_items(nq, [&](uint32_t i, bool valid) {
+        const uint32_t t = valid ? ldm(s.qa + i) : 0u;
+        const uint32_t rt = (valid && ranged) ? ldm(s.range + t) : 0u;
+        auto visit = [&](uint32_t, uint32_t u, uint32_t rtag) {
+          if (!live(u)) return;
+          if (ranged && ldm(s.range + u) != rtag) return;
+          if (bit_claim(s.queued, u)) queue_push(s.qb, cur() + C_Q2, s.qcap, u, err());
+        };
+        uint32_t b = valid ? ldg(g.off + t) : 0u, d = valid ? ldg(g.off + t + 1) - b : 0u;
+        warp_gather(t, b, d, rt, g.adj, visit);
+        b = valid ? ldg(g.offT + t) : 0u;
+        d = valid ? ldg(g.offT + t + 1) - b : 0u;
+        warp_gather(t, b, d, rt, g.adjT, visit);
+      });
+      if (!bar(101)) return it;
+      const uint32_t nc = rdprv(C_Q2);
+      ntrim = 0;
+      for_items(nc, [&](uint32_t i, bool valid) {
+        bool t = false;
+        uint32_t u = 0;
+        if (valid) {
+          u = ldm(s.qb + i);
+          bit_clear(s.queued, u);
+          if (live(u)) {
+            const uint32_t ru = ranged ? ldm(s.range + u) : 0u;
+            t = !live_nbr(g.off, g.adj, u, ru, ranged, false) || !live_nbr(g.offT, g.adjT, u, ru, ranged, false);
+            if (t) mark_trimmed(u);
+          }
+        }
+        warp_push(s.qa, cur() + C_Q, s.qcap, u, t, err());
+        ntrim += t;
+      });
+      add_count(&c->n_trimmed, ntrim);
+      if (!bar(102)) return it;
+      nq = rdprv(C_Q);
+      ++it;
+    }
+    return it;
+  }
+
+  // ===================================================== first pivot (a3)
+  // scc.cu:234-253: after the first trim the pivot is the first vertex that
+  // is not eliminated (or, with SCC_PIVOT_MAX_DEGREE, the one with the
+  // largest in x out degree).  Single partition only.
+  __device__ uint32_t pick_first_pivot() {
+    unsigned long long best = ~0ull;
+    for_vertices([&](uint32_t v, bool valid) {
+      if (valid && live(v)) {
+        const unsigned long long key = ((unsigned long long)prio(v) << 32) | v;
+        best = key < best ? key : best;
+      }
+    });
+    best = block_min_u64(best);
+    if (threadIdx.x == 0 && best != ~0ull) atomicMin(&c->best, best);
+    if (!bar(200)) return 0;
+    const unsigned long long b = ldm64(&c->best);
+    const uint32_t p = b == ~0ull ? 0u : (uint32_t)b;
+    // c->best is reset by the lead after the next barrier (everyone has read it by then)
+    if (is_lead()) {
+      if (p) {
+        P.s.rpivot[0] = p;
+        P.s.piv[0] = p;
+        bit_set(P.s.fvis, p);
+        bit_set(P.s.bvis, p);
+      }
+      c->piv_count = p ? 1u : 0u;
+    }
+    if (!bar(201)) return 0;
+    if (is_lead()) c->best = ~0ull;
+    return p;
+  }
+
+  // ======================================================== update (a13)
+  // scc_routines.cu:147-224: F∩B -> SCC of the partition's pivot; every other
+  // live vertex moves to partition (range, F, B); one pivot per non-empty new
+  // partition (smallest (priority, id)), which starts visited both ways.
+  // Also used for the first election when the graph is segmented (F = B = 0).
+  __device__ void update() {
+    const EngState &s = P.s;
+    __shared__ uint32_t s_key[kSlotCache];
+    __shared__ unsigned long long s_val[kSlotCache];
+    for (int i = threadIdx.x; i < kSlotCache; i += BS) {
+      s_key[i] = kNone;
+      s_val[i] = ~0ull;
+    }
+    __syncthreads();
+    uint32_t nelim = 0;
+    // A: eliminate F∩B, elect pivots (CTA-local min per key, flushed below)
+    for_vertices([&](uint32_t v, bool valid) {
+      uint32_t key = kNone;
+      unsigned long long val = ~0ull;
+      if (valid && live(v)) {
+        const bool f = bit_test(s.fvis, v), b = bit_test(s.bvis, v);
+        const uint32_t r = ldm(s.range + v);
+        if (f && b) {
+          s.label[v] = ldm(s.rpivot + r);
+          bit_set(s.elim, v);
+          ++nelim;
+        } else {
+          key = 3u * r + (f ? 1u : 0u) + (b ? 2u : 0u);
+          val = ((unsigned long long)prio(v) << 32) | v;
+        }
+      }
+      const uint32_t grp = __match_any_sync(kFull, key);
+      if (key != kNone) {
+        const uint32_t hi = (uint32_t)(val >> 32), lo = (uint32_t)val;
+        const uint32_t mhi = __reduce_min_sync(grp, hi);
+        const uint32_t mlo = __reduce_min_sync(grp, hi == mhi ? lo : kNone);
+        if (lane_id() == (uint32_t)(__ffs(grp) - 1)) {
+          const unsigned long long m = ((unsigned long long)mhi << 32) | mlo;
+          const uint32_t h = key % kSlotCache;
+          uint32_t owner = s_key[h];
+          if (owner == kNone) owner = atomicCAS(&s_key[h], kNone, key) == kNone ? key : s_key[h];
+          if (owner == key) {
+            atomicMin(&s_val[h], m);
+          } else if (ldm64(s.slot + key) > m) {
+            atomicMin(s.slot + key, m);
+          }
+        }
+      }
+    });
+    __syncthreads();
+    for (int i = threadIdx.x; i < kSlotCache; i += BS) {
+      const uint32_t key = s_key[i];
+      if (key != kNone && ldm64(s.slot + key) > s_val[i]) atomicMin(s.slot + key, s_val[i]);
+    }
+    add_count(&c->n_fbe, nelim);
+    if (!bar(300)) return;
+    // B: new partition id = elected pivot; pivots go to the pivot list
+    __shared__ unsigned long long s_hit[kSlotCache];  // (key << 32) | pivot
+    for (int i = threadIdx.x; i < kSlotCache; i += BS) s_hit[i] = ~0ull;
+    __syncthreads();
+    for_vertices([&](uint32_t v, bool valid) {
+      bool is_piv = false;
+      uint32_t key = 0;
+      if (valid && live(v)) {
+        const bool f = bit_test(s.fvis, v), b = bit_test(s.bvis, v);
+        key = 3u * ldm(s.range + v) + (f ? 1u : 0u) + (b ? 2u : 0u);
+        const uint32_t h = key % kSlotCache;
+        const unsigned long long cached = s_hit[h];
+        uint32_t np;
+        if ((uint32_t)(cached >> 32) == key) {
+          np = (uint32_t)cached;
+        } else {
+          np = (uint32_t)ldm64(s.slot + key);
+          s_hit[h] = ((unsigned long long)key << 32) | np;
+        }
+        s.range[v] = np;
+        is_piv = np == v;
+      }
+      const uint32_t mask = __ballot_sync(kFull, is_piv);
+      if (mask) {
+        const uint32_t leader = __ffs(mask) - 1;
+        uint32_t base = 0;
+        if (lane_id() == leader) base = atomicAdd(cur() + C_Q, __popc(mask));
+        base = __shfl_sync(kFull, base, leader);
+        if (is_piv) {
+          const uint32_t slot_i = base + __popc(mask & lanemask_lt());
+          s.piv[slot_i] = v;
+          s.pivkey[slot_i] = key;
+        }
+      }
+    });
+    if (!bar(301)) return;
+    const uint32_t np = rdprv(C_Q);
+    // C: release the election slots, clear the visit bitmaps
+    for_items(np, [&](uint32_t i, bool valid) {
+      if (valid) s.slot[ldm(s.pivkey + i)] = ~0ull;
+    });
+    for (uint32_t w = gtid(); w < s.nwords; w += gstride()) {
+      s.fvis[w] = 0u;
+      s.bvis[w] = 0u;
+      s.fexp[w] = 0u;
+      s.bexp[w] = 0u;
+    }
+    if (is_lead()) c->piv_count = np;
+    if (!bar(302)) return;
+    // D: pivots start F and B visited (state 19)
+    for_items(np, [&](uint32_t i, bool valid) {
+      if (valid) {
+        const uint32_t p = ldm(s.piv + i);
+        s.rpivot[p] = p;
+        bit_set(s.fvis, p);
+        bit_set(s.bvis, p);
+      }
+    });
+    bar(303);
+  }
+
+  // scc_routines.cu:10-19 unsetPivots: the pivots of the last election stop
+  // being pivots (their visit bits go), used right before WCC.
+  __device__ void unset_pivots() {
+    const EngState &s = P.s;
+    for (uint32_t w = gtid(); w < s.nwords; w += gstride()) {
+      s.fvis[w] = 0u;
+      s.bvis[w] = 0u;
+      s.fexp[w] = 0u;
+      s.bexp[w] = 0u;
+    }
+    if (is_lead()) c->piv_count = 0;
+    bar(400);
+  }
+
+  // ======================================================== reach (a8-a11)
+  // Visit predicate shared by every arm: u joins the visited set of the
+  // current direction when it is live, in the source's partition (unless
+  // first step) and not visited yet; exactly one caller wins the claim.
+  __device__ bool try_visit(uint32_t *vis, uint32_t u, bool ranged, uint32_t rsrc) {
+    if (bit_test(vis, u)) return false;
+    if (!live(u)) return false;
+    if (ranged && ldm(P.s.range + u) != rsrc) return false;
+    return bit_claim(vis, u);
+  }
+
+  // QUADRATIC (reach_q.cu:12-79,160-231): every sweep expands each visited,
+  // not yet expanded vertex, one thread per vertex.
+  __device__ uint32_t reach_q(const uint32_t *__restrict__ off, const uint32_t *__restrict__ adj, uint32_t *vis,
+                              uint32_t *exp, bool ranged) {
+    uint32_t depth = 0;
+    for (;;) {
+      uint32_t chg = 0;
+      for_vertices([&](uint32_t v, bool valid) {
+        if (!valid || !live(v) || !bit_test(vis, v) || bit_test(exp, v)) return;
+        bit_set(exp, v);
+        const uint32_t rv = ranged ? ldm(P.s.range + v) : 0u;
+        const uint32_t b = ldg(off + v), e = ldg(off + v + 1);
+        for (uint32_t i = b; i < e; ++i) chg += try_visit(vis, ldg(adj + i), ranged, rv);
+      });
+      add_count(cur() + C_CHG, chg);
+      if (!bar(500)) return depth;
+      ++depth;
+      if (rdprv(C_CHG) == 0) break;
+      if (depth >= P.o.max_iters) {
+        fail(kErrIterCap);
+        break;
+      }
+    }
+    return depth;
+  }
+
+  // Edges of lists longer than heavy_degree, collected during a push sweep
+  // and expanded afterwards by the whole grid in 256-edge chunks.
+  __device__ void heavy_push(uint32_t v, uint32_t beg, uint32_t deg, uint32_t tag) {
+    const unsigned long long old = atomicAdd(cur64(), (1ull << 32) | deg);
+    const uint32_t idx = (uint32_t)(old >> 32);
+    if (idx >= P.s.hcap) {
+      fail(kErrQueueOverflow);
+      return;
+    }
+    P.s.hv[idx] = v;
+    P.s.hbeg[idx] = beg;
+    P.s.hdeg[idx] = deg;
+    P.s.htag[idx] = tag;
+    P.s.hbase[idx] = (uint32_t)old;
+  }
+
+  template <class Visit>
+  __device__ void heavy_expand(const uint32_t *__restrict__ adj, unsigned long long h, Visit &&visit) {
+    const uint32_t cnt = (uint32_t)(h >> 32), tot = (uint32_t)h;
+    if (cnt == 0 || cnt > P.s.hcap) return;  // overflow already flagged by heavy_push
+    const EngState &s = P.s;
+    const uint32_t lane = lane_id();
+    for (uint32_t chunk = gwarp(); (unsigned long long)chunk * 256ull < tot; chunk += nwarps()) {
+      const uint32_t e0 = chunk * 256u;
+      uint32_t j = 0;
+      if (lane == 0) {  // largest j with hbase[j] <= e0
+        uint32_t lo = 0, hi = cnt - 1;
+        while (lo < hi) {
+          const uint32_t mid = (lo + hi + 1) >> 1;
+          if (ldm(s.hbase + mid) <= e0) lo = mid;
+          else hi = mid - 1;
+        }
+        j = lo;
+      }
+      j = __shfl_sync(kFull, j, 0);
+      for (uint32_t sft = 0; sft < 256u; sft += 32u) {
+        const uint32_t e = e0 + sft + lane;
+        if (e0 + sft >= tot) break;
+        if (e < tot) {
+          uint32_t jj = j;
+          while (jj + 1 < cnt && ldm(s.hbase + jj + 1) <= e) ++jj;
+          const uint32_t dst = ldg(adj + ldm(s.hbeg + jj) + (e - ldm(s.hbase + jj)));
+          visit(ldm(s.hv + jj), dst, ldm(s.htag + jj));
+        }
+      }
+    }
+  }
+
+  // TOPO / BEST (reach_t.cu): topology sweeps with warp-gather load
+  // balancing; when the frontier's edges exceed the unexplored edges / alpha
+  // a sweep pulls instead (every unvisited vertex scans its reverse list for
+  // a visited partition-mate) until the frontier falls under live / beta.
+  __device__ uint32_t reach_t(const uint32_t *__restrict__ off, const uint32_t *__restrict__ adj,
+                              const uint32_t *__restrict__ poff, const uint32_t *__restrict__ padj, uint32_t *vis,
+                              uint32_t *exp, bool ranged, bool allow_pull) {
+    const EngState &s = P.s;
+    uint32_t depth = 0;
+    bool pull = false;
+    unsigned long long nf = 1, mf = 0, explored = 0;
+    const unsigned long long mtot = P.g.m;
+    const uint32_t heavy = P.o.heavy_degree;
+    const long long alpha = P.o.pull_alpha > 0 ? P.o.pull_alpha : 14;
+    const long long beta = P.o.pull_beta > 0 ? P.o.pull_beta : 24;
+    for (;;) {
+      const uint32_t nlive = ldm(&c->n_live);
+      if (allow_pull) {
+        const unsigned long long unexplored = mtot > explored ? mtot - explored : 0ull;
+        if (!pull && depth > 0 && (long long)mf * alpha > (long long)unexplored) pull = true;
+        else if (pull && (long long)nf * beta < (long long)nlive) pull = false;
+      }
+      uint32_t chg = 0, degsum = 0;
+      auto visit = [&](uint32_t, uint32_t u, uint32_t rsrc) {
+        if (try_visit(vis, u, ranged, rsrc)) {
+          ++chg;
+          degsum += ldg(off + u + 1) - ldg(off + u);
+        }
+      };
+      if (!pull) {
+        for_vertices([&](uint32_t v, bool valid) {
+          const bool fr = valid && live(v) && bit_test(vis, v) && !bit_test(exp, v);
+          uint32_t b = 0, d = 0, rv = 0;
+          if (fr) {
+            bit_set(exp, v);
+            b = ldg(off + v);
+            d = ldg(off + v + 1) - b;
+            rv = ranged ? ldm(s.range + v) : 0u;
+            if (d > heavy) {
+              heavy_push(v, b, d, rv);
+              d = 0;
+            }
+          }
+          warp_gather(v, b, d, rv, adj, visit);
+        });
+        add_count(cur() + C_CHG, chg);
+        add_count(cur() + C_DEG, degsum);
+        if (!bar(600)) return depth;
+        const unsigned long long h = ldm64(prv64());
+        if ((uint32_t)(h >> 32) != 0) {
+          // carry the regular part's counts into this interval
+          if (is_lead()) {
+            atomicAdd(cur() + C_CHG, rdprv(C_CHG));
+            atomicAdd(cur() + C_DEG, rdprv(C_DEG));
+          }
+          chg = 0;
+          degsum = 0;
+          heavy_expand(adj, h, visit);
+          add_count(cur() + C_CHG, chg);
+          add_count(cur() + C_DEG, degsum);
+          if (!bar(601)) return depth;
+        }
+      } else {
+        if (is_lead()) atomicAdd(&c->pull_sweeps, 1u);
+        for_vertices([&](uint32_t v, bool valid) {
+          bool cand = false;
+          if (valid && live(v)) {
+            if (bit_test(vis, v)) {
+              if (!bit_test(exp, v)) bit_set(exp, v);  // reached before this sweep: its edges are covered
+            } else {
+              cand = true;
+            }
+          }
+          bool found = false;
+          if (cand) {
+            const uint32_t rv = ranged ? ldm(s.range + v) : 0u;
+            const uint32_t b = ldg(poff + v), e = ldg(poff + v + 1);
+            for (uint32_t i = b; i < e; ++i) {
+              const uint32_t u = ldg(padj + i);
+              if (bit_test(vis, u) && (!ranged || ldm(s.range + u) == rv)) {
+                found = true;
+                break;
+              }
+            }
+            if (found) {
+              bit_set(vis, v);
+              ++chg;
+              degsum += ldg(off + v + 1) - ldg(off + v);
+            }
+          }
+        });
+        add_count(cur() + C_CHG, chg);
+        add_count(cur() + C_DEG, degsum);
+        if (!bar(602)) return depth;
+      }
+      ++depth;
+      nf = rdprv(C_CHG);
+      mf = rdprv(C_DEG);
+      explored += mf;
+      if (nf == 0) break;
+      if (depth >= P.o.max_iters) {
+        fail(kErrIterCap);
+        break;
+      }
+    }
+    return depth;
+  }
+
+  // DATA / LINEAR (reach_d.cu, reach_l.cu): worklist levels seeded with the
+  // pivot list.  DATA expands one item per thread; LINEAR gathers the
+  // level's edges warp-wide and splits heavy lists across the grid.  Each
+  // vertex enters a worklist at most once (exactly-once claim), so the n-slot
+  // queues cannot overflow (reference worklistc.h:79-81 drops items).
+  __device__ uint32_t reach_wl(const uint32_t *__restrict__ off, const uint32_t *__restrict__ adj, uint32_t *vis,
+                               bool ranged, bool balanced) {
+    const EngState &s = P.s;
+    const uint32_t heavy = P.o.heavy_degree;
+    const uint32_t *in = s.piv;
+    uint32_t nin = ldm(&c->piv_count);
+    uint32_t *outs[2] = {s.qa, s.qb};
+    uint32_t depth = 0, sel = 0;
+    while (nin > 0) {
+      uint32_t *out = outs[sel];
+      uint32_t *cnt = cur() + C_Q;
+      uint32_t qoff = 0;  // items already appended to `out` in an earlier interval of this level
+      auto visit = [&](uint32_t, uint32_t u, uint32_t rsrc) {
+        if (try_visit(vis, u, ranged, rsrc)) queue_push(out + qoff, cnt, s.qcap - qoff, u, err());
+      };
+      if (balanced) {
+        for_items(nin, [&](uint32_t i, bool valid) {
+          uint32_t v = 0, b = 0, d = 0, rv = 0;
+          if (valid) {
+            v = ldm(in + i);
+            b = ldg(off + v);
+            d = ldg(off + v + 1) - b;
+            rv = ranged ? ldm(s.range + v) : 0u;
+            if (d > heavy) {
+              heavy_push(v, b, d, rv);
+              d = 0;
+            }
+          }
+          warp_gather(v, b, d, rv, adj, visit);
+        });
+        if (!bar(700)) return depth;
+        const unsigned long long h = ldm64(prv64());
+        if ((uint32_t)(h >> 32) != 0) {
+          qoff = rdprv(C_Q);
+          cnt = cur() + C_Q;
+          heavy_expand(adj, h, visit);
+          if (!bar(701)) return depth;
+          ++depth;
+          nin = qoff + rdprv(C_Q);
+          in = out;
+          sel ^= 1u;
+          if (depth >= P.o.max_iters) {
+            fail(kErrIterCap);
+            break;
+          }
+          continue;
+        }
+      } else {
+        for (uint32_t i = gtid(); i < nin; i += gstride()) {
+          const uint32_t v = ldm(in + i);
+          const uint32_t rv = ranged ? ldm(s.range + v) : 0u;
+          const uint32_t b = ldg(off + v), e = ldg(off + v + 1);
+          for (uint32_t j = b; j < e; ++j) visit(v, ldg(adj + j), rv);
+        }
+        if (!bar(702)) return depth;
+      }
+      ++depth;
+      nin = rdprv(C_Q);
+      in = out;
+      sel ^= 1u;
+      if (depth >= P.o.max_iters) {
+        fail(kErrIterCap);
+        break;
+      }
+    }
+    return depth;
+  }
+
+  __device__ uint32_t reach(uint32_t dir, uint32_t arm, bool ranged) {
+    const EngGraph &g = P.g;
+    const EngState &s = P.s;
+    const uint32_t *off = dir ? g.offT : g.off, *adj = dir ? g.adjT : g.adj;
+    const uint32_t *poff = dir ? g.off : g.offT, *padj = dir ? g.adj : g.adjT;
+    uint32_t *vis = dir ? s.bvis : s.fvis, *exp = dir ? s.bexp : s.fexp;
+    switch (arm) {
+      case ARM_Q: return reach_q(off, adj, vis, exp, ranged);
+      case ARM_D: return reach_wl(off, adj, vis, ranged, false);
+      case ARM_L: return reach_wl(off, adj, vis, ranged, true);
+      case ARM_B: return reach_t(off, adj, poff, padj, vis, exp, ranged, true);
+      default: return reach_t(off, adj, poff, padj, vis, exp, ranged, P.o.pull_alpha >= 0);
+    }
+  }
+
+  // ========================================================== trim-2 (a7)
+  // scc_routines.cu:397-523: v whose only live partition-mate out-neighbour
+  // u has v as its only live partition-mate out-neighbour (or the same with
+  // in-neighbours) forms the 2-vertex SCC {v, u}; the smaller id is its
+  // representative (states 20 / 4).  Detection reads a snapshot (no
+  // eliminations until every vertex has been examined), so the result does
+  // not depend on thread order.
+  __device__ uint32_t single_live(const uint32_t *__restrict__ off, const uint32_t *__restrict__ adj, uint32_t v,
+                                  uint32_t rv) {
+    const uint32_t b = ldg(off + v), e = ldg(off + v + 1);
+    uint32_t found = kNone, n = 0;
+    for (uint32_t i = b; i < e; ++i) {
+      const uint32_t u = ldg(adj + i);
+      if (u == v || !live(u) || ldm(P.s.range + u) != rv) continue;
+      if (++n > 1) return kNone;
+      found = u;
+    }
+    return found;
+  }
+  __device__ bool only_to(const uint32_t *__restrict__ off, const uint32_t *__restrict__ adj, uint32_t u, uint32_t v,
+                          uint32_t rv) {
+    const uint32_t b = ldg(off + u), e = ldg(off + u + 1);
+    uint32_t n = 0;
+    for (uint32_t i = b; i < e; ++i) {
+      const uint32_t w = ldg(adj + i);
+      if (w == u || !live(w) || ldm(P.s.range + w) != rv) continue;
+      if (w != v) return false;
+      ++n;
+    }
+    return n == 1;
+  }
+  __device__ uint32_t trim2() {
+    const EngState &s = P.s;
+    const EngGraph &g = P.g;
+    for_vertices([&](uint32_t v, bool valid) {
+      if (!valid || !live(v)) return;
+      const uint32_t rv = ldm(s.range + v);
+      uint32_t u = single_live(g.off, g.adj, v, rv);
+      bool pair = u != kNone && only_to(g.off, g.adj, u, v, rv);
+      if (!pair) {
+        u = single_live(g.offT, g.adjT, v, rv);
+        pair = u != kNone && only_to(g.offT, g.adjT, u, v, rv);
+      }
+      if (pair) {
+        s.aux[v] = u;
+        bit_set(s.queued, v);
+      }
+    });
+    if (!bar(800)) return 0;
+    uint32_t cnt = 0;
+    for_vertices([&](uint32_t v, bool valid) {
+      if (!valid || !bit_test(s.queued, v)) return;
+      const uint32_t u = ldm(s.aux + v);
+      s.label[v] = u < v ? u : v;
+      bit_set(s.elim, v);
+      bit_clear(s.queued, v);
+      ++cnt;
+    });
+    add_count(&c->n_trim2, cnt);
+    add_count(cur() + C_CNT, cnt);
+    if (!bar(801)) return 0;
+    return rdprv(C_CNT);
+  }
+
+  // ============================================================= WCC (a15)
+  // wcc.cu:7-52,79-144: colour = smallest id reachable through out-edges
+  // inside the partition (min-label propagation plus pointer jumping, to a
+  // fixpoint); each colour becomes a partition whose pivot is the colour's
+  // root.  The colour is constant on an SCC, so no SCC is split.
+  __device__ uint32_t wcc() {
+    const EngState &s = P.s;
+    const EngGraph &g = P.g;
+    uint32_t *lab = s.aux;
+    for_vertices([&](uint32_t v, bool valid) {
+      if (valid && live(v)) lab[v] = v;
+    });
+    if (!bar(900)) return 0;
+    uint32_t it = 0;
+    for (;;) {
+      uint32_t chg = 0;
+      for_vertices([&](uint32_t v, bool valid) {
+        if (!valid || !live(v)) return;
+        const uint32_t old = ldm(lab + v);
+        uint32_t m = old;
+        const uint32_t rv = ldm(s.range + v);
+        const uint32_t b = ldg(g.off + v), e = ldg(g.off + v + 1);
+        for (uint32_t i = b; i < e; ++i) {
+          const uint32_t u = ldg(g.adj + i);
+          if (!live(u) || ldm(s.range + u) != rv) continue;
+          const uint32_t x = ldm(lab + u);
+          m = x < m ? x : m;
+        }
+        const uint32_t j = ldm(lab + m);
+        m = j < m ? j : m;
+        if (m < old) {
+          lab[v] = m;
+          ++chg;
+        }
+      });
+      add_count(cur() + C_CHG, chg);
+      if (!bar(901)) return it;
+      ++it;
+      if (rdprv(C_CHG) == 0) break;
+      if (it >= P.o.max_iters) {
+        fail(kErrIterCap);
+        break;
+      }
+    }
+    // roots become pivots of fresh partitions; members join their root's
+    for_vertices([&](uint32_t v, bool valid) {
+      bool root = false;
+      if (valid && live(v)) {
+        const uint32_t r = ldm(lab + v);
+        s.range[v] = r;
+        root = r == v;
+        if (root) s.rpivot[v] = v;
+      }
+      warp_push(s.piv, cur() + C_Q, s.qcap, v, root, err());
+    });
+    if (!bar(902)) return it;
+    const uint32_t np = rdprv(C_Q);
+    for_items(np, [&](uint32_t i, bool valid) {
+      if (valid) {
+        const uint32_t p = ldm(s.piv + i);
+        bit_set(s.fvis, p);
+        bit_set(s.bvis, p);
+      }
+    });
+    if (is_lead()) c->piv_count = np;
+    bar(903);
+    return it;
+  }
+
+  // ============================================= active-list compaction
+  __device__ void compact() {
+    const EngState &s = P.s;
+    uint32_t *dst = s.act[act_sel ^ 1u];
+    for_vertices([&](uint32_t v, bool valid) {
+      const bool a = valid && live(v);
+      warp_push(dst, cur() + C_Q, s.qcap, v, a, err());
+    });
+    if (!bar(1000)) return;
+    if (is_lead()) {
+      c->act_count = rdprv(C_Q);
+      c->act_sel = act_sel ^ 1u;
+      c->list_mode = 1;
+    }
+    if (!bar(1001)) return;
+    refresh_mode();
+  }
+
+  __device__ void maybe_compact() {
+    const uint32_t nlive = ldm(&c->n_live);
+    const uint32_t span = list_mode ? act_count : P.g.n;
+    if ((unsigned long long)nlive * 4ull < span) compact();
+  }
+
+  __device__ void sync_live() {
+    // n_live = n - trimmed - trim2 - F∩B; every CTA computes the same value
+    if (is_lead()) {
+      const uint32_t gone = ldm(&c->n_trimmed) + ldm(&c->n_trim2) + ldm(&c->n_fbe);
+      c->n_live = P.g.n - gone;
+    }
+  }
+
+  // ================================================== finalize labels
+  __device__ void finalize() {
+    const EngState &s = P.s;
+    list_mode = 0;
+    if (P.o.pivot_rule != 0) {  // representatives are pivots: canonicalise to min id
+      for_all_ids([&](uint32_t v, bool valid) {
+        if (valid) s.aux[v] = kNone;
+      });
+      if (!bar(1100)) return;
+      for_all_ids([&](uint32_t v, bool valid) {
+        const uint32_t l = valid ? ldm(s.label + v) : kNone;
+        const uint32_t grp = __match_any_sync(kFull, l);
+        if (valid) {
+          const uint32_t mn = __reduce_min_sync(grp, v);
+          if (lane_id() == (uint32_t)(__ffs(grp) - 1) && l != 0) atomicMin(s.aux + l, mn);
+        }
+      });
+      if (!bar(1101)) return;
+      for_all_ids([&](uint32_t v, bool valid) {
+        if (valid) {
+          const uint32_t l = ldm(s.label + v);
+          if (l != 0) s.label[v] = ldm(s.aux + l);
+        }
+      });
+      if (!bar(1102)) return;
+    }
+    uint32_t cnt = 0, unresolved = 0;
+    for_all_ids([&](uint32_t v, bool valid) {
+      if (!valid) return;
+      const uint32_t l = ldm(s.label + v);
+      cnt += l == v;
+      unresolved += l == 0;
+      if (s.out_labels) s.out_labels[v] = l;
+    });
+    if (s.out_labels && is_lead()) s.out_labels[0] = 0;
+    add_count(cur() + C_CNT, cnt);
+    add_count(cur() + C_CNT2, unresolved);
+    if (!bar(1103)) return;
+    if (is_lead()) {
+      c->nscc = rdprv(C_CNT);
+      c->phase_ret = rdprv(C_CNT2);
+    }
+  }
+
+  // ================================================= the driver (a3)
+  __device__ void timed(unsigned long long &acc, unsigned long long t0) {
+    if (is_lead()) acc += globaltimer_ns() - t0;
+  }
+
+  __device__ uint32_t arm_for(bool below) const {
+    switch (P.o.alg) {
+      case 0: return ARM_Q;
+      case 1: return ARM_T;
+      case 2: return ARM_D;
+      case 3: return ARM_L;
+      case 4: return below ? ARM_T : ARM_Q;  // HYBRID: reach_t below n/100, reach_q above
+      case 5: return below ? ARM_L : ARM_Q;  // COMBINE
+      case 6: return below ? ARM_B : ARM_Q;  // BEST
+      default: return ARM_T;
+    }
+  }
+
+  __device__ void solve() {
+    const EngOpts &o = P.o;
+    const bool single = P.s.nseg <= 1;
+    refresh_mode();
+    unsigned long long t0 = globaltimer_ns();
+    if (o.trim_first) {
+      const uint32_t it = trim(false, P.g.sorted_unique != 0, o.max_iters);
+      if (is_lead()) c->trim_iters += it;
+      sync_live();
+      if (!bar(1)) return;
+    }
+    timed(c->ns_trim, t0);
+    t0 = globaltimer_ns();
+    if (single) {
+      pick_first_pivot();
+    } else {
+      update();
+      sync_live();
+      if (!bar(2)) return;
+    }
+    timed(c->ns_update, t0);
+    uint32_t step = 0;
+    bool wcc_done = false;  // CTA-uniform: every CTA takes the WCC branch in the same round
+    while (ldm(&c->piv_count) > 0) {
+      if (ldm(&c->gs.err)) return;
+      ++step;
+      if (step > o.max_iters) {
+        fail(kErrIterCap);
+        return;
+      }
+      const uint32_t nel = ldm(&c->n_fbe) + ldm(&c->n_trim2);
+      const uint32_t arm = arm_for(nel < o.switch_thr);
+      const bool ranged = !(step == 1 && single);
+      t0 = globaltimer_ns();
+      const uint32_t fd = reach(0, arm, ranged);
+      timed(c->ns_fwd, t0);
+      t0 = globaltimer_ns();
+      const uint32_t bd = reach(1, arm, ranged);
+      timed(c->ns_bwd, t0);
+      t0 = globaltimer_ns();
+      uint32_t ti = 0;
+      if (o.trim_depth >= 0) {
+        const uint32_t cap = o.trim_depth == 0 ? o.max_iters : (uint32_t)o.trim_depth;
+        ti = trim(ranged, false, cap);
+      }
+      sync_live();
+      if (!bar(3)) return;
+      timed(c->ns_trim, t0);
+      t0 = globaltimer_ns();
+      update();
+      sync_live();
+      if (!bar(4)) return;
+      timed(c->ns_update, t0);
+      if (is_lead()) {
+        c->steps = step;
+        c->fwd_depth += fd;
+        c->bwd_depth += bd;
+        c->trim_iters += ti;
+      }
+      if (o.wcc && !wcc_done) {
+        const uint32_t nel2 = ldm(&c->n_fbe) + ldm(&c->n_trim2);
+        if (nel2 >= o.switch_thr) {
+          t0 = globaltimer_ns();
+          wcc_done = true;
+          if (is_lead()) {
+            c->wcc_done = 1;
+            c->wcc_step = step;
+          }
+          if (ldm(&c->n_live) > 0) {
+            unset_pivots();
+            if (o.trim2) {
+              trim2();
+              sync_live();
+              if (!bar(5)) return;
+            }
+            const uint32_t wi = wcc();
+            if (is_lead()) c->wcc_iters += wi;
+          }
+          timed(c->ns_wcc, t0);
+        }
+      }
+      maybe_compact();
+      if (!bar(6)) return;
+    }
+    finalize();
+  }
+};
+
+// ------------------------------------------------------------------ kernels
+template <int BS>
+__global__ void __launch_bounds__(BS, 1024 / BS) scc_persistent(Params p, uint32_t phase, uint32_t a0, uint32_t a1,
+                                                                 uint32_t a2) {
+  Eng<BS> e(p);
+  Ctl *c = p.s.ctl;
+  e.refresh_mode();
+  switch (phase) {
+    case PH_SOLVE: e.solve(); break;
+    case PH_TRIM1: {
+      const bool snap = p.g.sorted_unique && ldm(&c->n_live) == p.g.n;
+      const uint32_t it = e.trim(false, snap, p.o.max_iters);
+      e.sync_live();
+      if (e.is_lead()) c->phase_ret = it;
+      break;
+    }
+    case PH_TRIM: {
+      const uint32_t it = e.trim(true, false, p.o.max_iters);
+      e.sync_live();
+      if (e.is_lead()) c->phase_ret = it;
+      break;
+    }
+    case PH_TRIM2: {
+      const uint32_t r = e.trim2();
+      e.sync_live();
+      if (e.is_lead()) c->phase_ret = r;
+      break;
+    }
+    case PH_SELECT:
+      if (p.s.nseg <= 1) {
+        e.pick_first_pivot();
+      } else {
+        e.update();
+        e.sync_live();
+      }
+      break;
+    case PH_REACH: {
+      const uint32_t d = e.reach(a0, a1, a2 != 0);
+      if (e.is_lead()) c->phase_ret = d;
+      break;
+    }
+    case PH_UPDATE:
+      e.update();
+      e.sync_live();
+      break;
+    case PH_UNSET: e.unset_pivots(); break;
+    case PH_WCC: {
+      const uint32_t it = e.wcc();
+      if (e.is_lead()) c->phase_ret = it;
+      break;
+    }
+    case PH_FINALIZE: e.finalize(); break;
+    default: break;
+  }
+}
+
+// per-solve reset: labels, partitions (segment index or 0), bitmaps
+__global__ void scc_init_kernel(Params p) {
+  const uint32_t n = p.g.n;
+  const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
+  for (uint32_t v = tid; v <= n; v += stride) {
+    p.s.label[v] = 0;
+    uint32_t r = 0;
+    if (p.s.nseg > 1 && v >= 1) {
+      uint32_t lo = 0, hi = p.s.nseg - 1;  // largest s with seg[s] <= v
+      while (lo < hi) {
+        const uint32_t mid = (lo + hi + 1) >> 1;
+        if (p.s.seg[mid] <= v) lo = mid;
+        else hi = mid - 1;
+      }
+      r = lo;
+    }
+    p.s.range[v] = r;
+  }
+  for (uint32_t w = tid; w < p.s.nwords; w += stride) {
+    uint32_t e = 0;
+    const uint32_t lo = w * 32u;
+    for (uint32_t b = 0; b < 32; ++b) {
+      const uint32_t v = lo + b;
+      if (v == 0 || v > n) e |= 1u << b;
+    }
+    p.s.elim[w] = e;
+    p.s.fvis[w] = 0;
+    p.s.bvis[w] = 0;
+    p.s.fexp[w] = 0;
+    p.s.bexp[w] = 0;
+    p.s.tflag[w] = 0;
+    p.s.queued[w] = 0;
+  }
+  if (tid == 0) {
+    p.s.ctl->best = ~0ull;
+    p.s.ctl->n_live = n;
+  }
+}
+
+__global__ void scc_states_kernel(Params p, uint8_t *out) {
+  const uint32_t n = p.g.n;
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v <= n; v += gridDim.x * blockDim.x) {
+    if (v == 0) {
+      out[0] = 0;
+      continue;
+    }
+    auto bit = [&](const uint32_t *bm) { return (bm[v >> 5] >> (v & 31u)) & 1u; };
+    const bool e = v <= n && bit(p.s.elim) && v != 0;
+    uint8_t st = 0;
+    if (bit(p.s.bvis)) st |= 1;
+    if (bit(p.s.fvis)) st |= 2;
+    if (e) st |= 4;
+    if (bit(p.s.tflag)) st |= 8;
+    if (e && p.s.label[v] == v) st |= 16;
+    if (!e && (st & 3) == 3 && p.s.rpivot[p.s.range[v]] == v) st |= 16;  // live pivot (state 19)
+    out[v] = st;
+  }
+}
+
+// CSR sanity for caller-provided device graphs: offsets start at 0, never
+// decrease and end at m; every neighbour id lies in 1..n.  Offsets are
+// checked in a first launch so the second only reads inside adj[0, m).
+__global__ void scc_check_offsets_kernel(const uint32_t *off, uint32_t n, uint32_t m, uint32_t *bad) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x + 1; v <= n; v += gridDim.x * blockDim.x) {
+    const uint32_t a = off[v], b = off[v + 1];
+    if (a > b || b > m || (v == 1 && a != 0) || (v == n && b != m)) atomicOr(bad, 1u);
+  }
+}
+__global__ void scc_check_edges_kernel(const uint32_t *adj, uint32_t n, uint32_t m, uint32_t *bad) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
+    const uint32_t u = adj[i];
+    if (u < 1 || u > n) atomicOr(bad, 2u);
+  }
+}
+
+cudaError_t check_device_csr(const uint32_t *off, const uint32_t *adj, uint32_t n, uint32_t m, uint32_t *d_bad,
+                             uint32_t *h_bad, cudaStream_t st) {
+  cudaError_t e = cudaMemsetAsync(d_bad, 0, 4, st);
+  if (e != cudaSuccess) return e;
+  if (n) scc_check_offsets_kernel<<<148 * 4, 256, 0, st>>>(off, n, m, d_bad);
+  e = cudaMemcpyAsync(h_bad, d_bad, 4, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess || *h_bad) return e;
+  if (m) scc_check_edges_kernel<<<148 * 8, 256, 0, st>>>(adj, n, m, d_bad);
+  e = cudaMemcpyAsync(h_bad, d_bad, 4, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  return e;
+}
+
+__global__ void scc_ranges_kernel(Params p, uint32_t *out) {
+  const uint32_t n = p.g.n;
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v <= n; v += gridDim.x * blockDim.x) {
+    const bool e = v == 0 || ((p.s.elim[v >> 5] >> (v & 31u)) & 1u);
+    out[v] = e ? 0u : p.s.range[v];
+  }
+}
+
+template <int BS>
+static cudaError_t coop_launch(const Params &p, uint32_t phase, uint32_t a0, uint32_t a1, uint32_t a2,
+                               uint32_t grid_blocks, cudaStream_t stream, uint32_t *grid_used) {
+  int dev = 0, sms = 0, per_sm = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (e != cudaSuccess) return e;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, scc_persistent<BS>, BS, 0);
+  if (e != cudaSuccess) return e;
+  if (per_sm < 1) return cudaErrorInvalidConfiguration;
+  uint32_t maxg = (uint32_t)(sms * per_sm);
+  uint32_t g = grid_blocks ? (grid_blocks < maxg ? grid_blocks : maxg) : maxg;
+  if (grid_used) *grid_used = g;
+  Params pp = p;
+  void *args[] = {&pp, &phase, &a0, &a1, &a2};
+  return cudaLaunchCooperativeKernel((const void *)scc_persistent<BS>, dim3(g), dim3(BS), args, 0, stream);
+}
+
+cudaError_t launch_phase(const Params &p, uint32_t phase, uint32_t a0, uint32_t a1, uint32_t a2, int block_size,
+                         uint32_t grid_blocks, cudaStream_t stream, uint32_t *grid_used) {
+  switch (block_size) {
+    case 128: return coop_launch<128>(p, phase, a0, a1, a2, grid_blocks, stream, grid_used);
+    case 512: return coop_launch<512>(p, phase, a0, a1, a2, grid_blocks, stream, grid_used);
+    case 1024: return coop_launch<1024>(p, phase, a0, a1, a2, grid_blocks, stream, grid_used);
+    default: return coop_launch<256>(p, phase, a0, a1, a2, grid_blocks, stream, grid_used);
+  }
+}
+
+cudaError_t persistent_grid(int block_size, uint32_t *grid_blocks) {
+  int dev = 0, sms = 0, per_sm = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (e != cudaSuccess) return e;
+  switch (block_size) {
+    case 128: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, scc_persistent<128>, 128, 0); break;
+    case 512: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, scc_persistent<512>, 512, 0); break;
+    case 1024: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, scc_persistent<1024>, 1024, 0); break;
+    default: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, scc_persistent<256>, 256, 0); break;
+  }
+  if (e != cudaSuccess) return e;
+  *grid_blocks = (uint32_t)(sms * per_sm);
+  return cudaSuccess;
+}
+
+cudaError_t launch_init(const Params &p, cudaStream_t stream) {
+  const uint32_t work = p.g.n + 1 > p.s.nwords ? p.g.n + 1 : p.s.nwords;
+  uint32_t blocks = (work + 255) / 256;
+  if (blocks > 148u * 16u) blocks = 148u * 16u;
+  if (blocks == 0) blocks = 1;
+  scc_init_kernel<<<blocks, 256, 0, stream>>>(p);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_states(const Params &p, uint8_t *d_states, cudaStream_t stream) {
+  uint32_t blocks = (p.g.n + 256) / 256;
+  if (blocks > 148u * 16u) blocks = 148u * 16u;
+  scc_states_kernel<<<blocks, 256, 0, stream>>>(p, d_states);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_ranges(const Params &p, uint32_t *d_ranges, cudaStream_t stream) {
+  uint32_t blocks = (p.g.n + 256) / 256;
+  if (blocks > 148u * 16u) blocks = 148u * 16u;
+  scc_ranges_kernel<<<blocks, 256, 0, stream>>>(p, d_ranges);
+  return cudaGetLastError();
+}
+
+}  // namespace sccb

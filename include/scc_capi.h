@@ -1,0 +1,250 @@
+/*
+ * scc_capi.h — C ABI of the B200 strongly-connected-components engine.
+ *
+ * The reference (chenxuhao/gpuscc_code) exposes its hot path as C++ host
+ * functions with C++ linkage (overloads on bool* / Worklist2*, alg_opt by
+ * value, errors abort the process).  Every entry point below replaces one of
+ * them with a plain C symbol: plain pointers and sizes, an int status
+ * (0 = SCC_OK, negative = error, text from scc_last_error()), no exit().
+ *
+ * Graph conventions follow the reference exactly (load.cpp:125-197):
+ *   vertex ids are 1..n, slot 0 is unused;
+ *   nodes[n+2]: out-edges of v are edges[nodes[v] .. nodes[v+1]), nodes[1] = 0;
+ *   nodesT/edgesT: the transpose (in-edges), same layout;
+ *   edges hold 1-based vertex ids.
+ * Labels: labels[v] (v = 1..n) is the smallest vertex id of v's strongly
+ * connected component; labels[0] = 0.
+ *
+ * Thread safety: one context per host thread (each context owns one CUDA
+ * stream); different contexts may be used concurrently.
+ */
+#ifndef GPUSCC_B200_SCC_CAPI_H
+#define GPUSCC_B200_SCC_CAPI_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- status */
+#define SCC_OK 0
+#define SCC_ERR_INVALID (-1)   /* bad argument */
+#define SCC_ERR_IO (-2)        /* file missing / unparsable */
+#define SCC_ERR_NOMEM (-3)     /* host or device allocation failed */
+#define SCC_ERR_CUDA (-4)      /* CUDA runtime error */
+#define SCC_ERR_TIMEOUT (-5)   /* a device-side bounded wait or iteration cap ran out */
+#define SCC_ERR_NODEVICE (-6)  /* no CUDA device */
+#define SCC_ERR_STATE (-7)     /* call out of order (e.g. phase before scc_phase_begin) */
+#define SCC_ERR_CAPACITY (-8)  /* graph exceeds the 32-bit id / offset range or a fixed limit */
+#define SCC_ERR_BUSY (-9)      /* server: request not finished yet */
+#define SCC_ERR_REJECTED (-10) /* server: admission refused (does not fit in device memory) */
+
+/* Message of the last error raised on this host thread ("" if none). */
+const char *scc_last_error(void);
+/* Library version string. */
+const char *scc_version(void);
+
+/* -------------------------------------------------------------- options */
+/* Reachability strategies; values equal the reference enum reach_strategy
+ * (scc.h:7-16) so the -a flag maps one to one. */
+enum scc_alg {
+  SCC_ALG_QUADRATIC = 0, /* -a q: topology sweep, one thread per vertex     (reach_q.cu) */
+  SCC_ALG_TOPO = 1,      /* -a t: topology sweep, warp-gather load balance  (reach_t.cu) */
+  SCC_ALG_DATA = 2,      /* -a d: data-driven worklist, thread per item     (reach_d.cu) */
+  SCC_ALG_LINEAR = 3,    /* -a l: data-driven worklist, degree-binned gather (reach_l.cu) */
+  SCC_ALG_HYBRID = 4,    /* -a h: TOPO until switch point, then QUADRATIC  (scc.cu:493-563) */
+  SCC_ALG_COMBINE = 5,   /* -a c: LINEAR until switch point, then QUADRATIC (scc.cu:565-638) */
+  SCC_ALG_BEST = 6       /* -a b: TOPO with pull sweeps until switch, then QUADRATIC (scc.cu:641-703) */
+};
+
+enum scc_pivot_rule {
+  SCC_PIVOT_MIN_ID = 0,    /* smallest active id of the partition (reference: first id, scc.cu:235-245) */
+  SCC_PIVOT_MAX_DEGREE = 1 /* largest in-degree x out-degree, ties to the smaller id */
+};
+
+typedef struct scc_opts {
+  int32_t alg;             /* enum scc_alg (reference default TOPO, scc.cu:80) */
+  int32_t wcc;             /* 1: WCC colouring once after the first big elimination (-DWCC, scc_w) */
+  int32_t trim2;           /* 1: trim-2 once together with WCC (-DTRIM_2, scc_2_w) */
+  int32_t trim_first;      /* 1: global trim-1 fixpoint before the first pivot (TRIM_FIRST, scc.cu:38) */
+  int32_t block_size;      /* threads per block of the persistent kernels (0 = 256); -b */
+  int32_t warp_size;       /* accepted for -w compatibility, not used (alg_opt.warp_size is never read) */
+  int32_t pivot_rule;      /* enum scc_pivot_rule */
+  int32_t switch_permille; /* hybrid/combine/best/WCC switch: eliminated >= n*permille/1000 (reference 10 = n/100) */
+  int32_t trim_depth;      /* per-round range-aware trim-1: 0 = to fixpoint, k > 0 = at most k iterations, -1 = off */
+  int32_t pull_alpha;      /* TOPO/BEST push->pull switch: frontier edges > unexplored edges / alpha (0 = 14) */
+  int32_t pull_beta;       /* pull->push switch: newly reached < active / beta (0 = 24) */
+  uint32_t warp_degree;    /* adjacency length from which a list is expanded by a whole warp (0 = 32) */
+  uint32_t heavy_degree;   /* adjacency length from which a list is split across the grid (0 = 4096) */
+  uint32_t max_iters;      /* cap on sweeps of any one fixpoint/reach loop and on FB rounds (0 = 1<<20) */
+  uint32_t grid_blocks;    /* persistent grid size (0 = every co-resident block) */
+  uint32_t timeout_ms;     /* bound on any device-side wait inside the persistent kernel (0 = 10000) */
+} scc_opts;
+
+/* Reference defaults: alg TOPO, wcc 0, trim2 0, trim_first 1, block 256, pivot MIN_ID, switch 10. */
+void scc_opts_default(scc_opts *opts);
+
+/* ----------------------------------------------------------- host graph */
+typedef struct scc_host_csr {
+  uint32_t n;          /* countOfNodes */
+  uint32_t m;          /* stored (deduplicated) edges = nodes[n+1] */
+  uint32_t nnz_header; /* countOfEdges as load() reports it (header nnz; + extra for symmetric) */
+  int32_t symmetric;   /* 1: nodesT == nodes, edgesT == edges (MatrixMarket "symmetric") */
+  int32_t sorted_unique; /* 1: every adjacency list is strictly increasing (load() guarantees it) */
+  int32_t owned;       /* 1: arrays were allocated by this library (scc_host_csr_free frees them) */
+  uint32_t *nodes;     /* n+2 */
+  uint32_t *edges;     /* m (+1 slack) */
+  uint32_t *nodesT;    /* n+2 */
+  uint32_t *edgesT;    /* m (+1 slack) */
+} scc_host_csr;
+
+/* load.h:5 / load.cpp:18 `bool load(char*, bool header, unsigned* countOfNodes,
+ * unsigned* countOfEdges, unsigned** nodes, unsigned** edges, unsigned** nodesT,
+ * unsigned** edgesT, unsigned*, unsigned*)`.  Same text / MatrixMarket format:
+ * first line checked for "pattern" / "symmetric", '%' comment lines skipped,
+ * header "m n nnz" for *.mtx (m must equal n) else "n nnz", each edge line is
+ * "dst src [w]" giving the edge src->dst, symmetric files add both directions,
+ * duplicates merged, neighbours sorted, self-loops kept.  `header` is accepted
+ * and ignored exactly like the reference.  Parses with sort+unique instead of
+ * std::set.  Returns SCC_ERR_IO instead of exit(1). */
+int scc_load(const char *path, int header, scc_host_csr *out);
+void scc_host_csr_free(scc_host_csr *csr);
+/* Build a host CSR (+transpose) from an edge list of 1-based (src, dst) pairs:
+ * duplicates merged, lists sorted, self-loops kept unless drop_self_loops. */
+int scc_csr_from_edges(uint32_t n, uint64_t n_edges, const uint32_t *src, const uint32_t *dst,
+                       int drop_self_loops, scc_host_csr *out);
+
+/* tarjan.h:5 / tarjan.cpp:72 `TR_Decomposition(CSize, RSize, Fc, Fr)`: the CPU
+ * decomposition behind the apps' -t flag (sequential, one host thread).
+ * labels: optional (n+1) output, canonical min-id labels.  secs: wall time. */
+int scc_tarjan(const scc_host_csr *csr, uint32_t *labels, uint32_t *nscc, double *secs);
+
+/* --------------------------------------------------------- synthetic graphs
+ * Deterministic generators (counter-based hashing: identical output for the
+ * same arguments on any machine and on the device).  All produce deduplicated
+ * sorted CSR + transpose with self-loops removed. */
+/* R-MAT, n = 2^scale, `samples` edge draws, (a,b,c,d) given in parts per
+ * million, vertex ids permuted by a seeded bijection when permute != 0. */
+int scc_gen_rmat(uint32_t scale, uint64_t samples, uint32_t a_ppm, uint32_t b_ppm, uint32_t c_ppm,
+                 uint64_t seed, int permute, scc_host_csr *out);
+/* Erdos-Renyi style: `samples` uniform directed draws over n vertices. */
+int scc_gen_er(uint32_t n, uint64_t samples, uint64_t seed, scc_host_csr *out);
+/* side x side grid, each undirected grid edge oriented by a coin flip,
+ * bidir_ppm of them made bidirectional, plus floor(grid_edges*longrange_ppm/1e6)
+ * uniform random directed long-range edges. */
+int scc_gen_grid(uint32_t side, uint32_t bidir_ppm, uint32_t longrange_ppm, uint64_t seed,
+                 scc_host_csr *out);
+
+/* ---------------------------------------------------------- device graph */
+typedef struct scc_dev_csr {
+  uint32_t n, m;
+  int32_t sorted_unique;
+  const uint32_t *nodes, *edges, *nodesT, *edgesT; /* device pointers, reference layout */
+} scc_dev_csr;
+
+/* Same R-MAT graph as scc_gen_rmat, generated, sorted and laid out on the
+ * device of `ctx` (the 2^26-vertex / 2^30-sample graph does not fit a host
+ * std::sort budget).  The arrays are owned by ctx and bound as its graph. */
+typedef struct scc_ctx scc_ctx;
+int scc_gen_rmat_device(scc_ctx *ctx, uint32_t scale, uint64_t samples, uint32_t a_ppm,
+                        uint32_t b_ppm, uint32_t c_ppm, uint64_t seed, int permute,
+                        scc_dev_csr *out);
+
+/* --------------------------------------------------------------- context */
+int scc_ctx_create(int device, const scc_opts *opts, scc_ctx **out);
+int scc_ctx_destroy(scc_ctx *ctx);
+int scc_ctx_set_opts(scc_ctx *ctx, const scc_opts *opts);
+int scc_ctx_get_opts(const scc_ctx *ctx, scc_opts *opts);
+/* cudaStream_t the context launches on. */
+void *scc_ctx_stream(scc_ctx *ctx);
+/* Copy a host graph into context-owned device buffers (grown on demand). */
+int scc_ctx_upload(scc_ctx *ctx, const scc_host_csr *csr);
+/* Use a caller-owned device graph (borrowed; must outlive its use). */
+int scc_ctx_bind_device(scc_ctx *ctx, const scc_dev_csr *csr);
+/* Copy the bound graph back to the host (for the apps' -t and for tests). */
+int scc_ctx_download(scc_ctx *ctx, scc_host_csr *out);
+/* Independent graphs packed in one CSR (batching): segment s owns vertices
+ * seg_first[s] .. seg_first[s+1]-1 (1-based, seg_first[0] = 1,
+ * seg_first[nseg] = n+1; no edge may cross segments).  nseg = 0 clears. */
+int scc_ctx_set_segments(scc_ctx *ctx, uint32_t nseg, const uint32_t *seg_first);
+
+typedef struct scc_stats {
+  uint32_t steps;          /* FB rounds (scc.cu:998 "steps") */
+  uint32_t fwd_depth;      /* sum of forward reach sweeps (scc.cu:999) */
+  uint32_t bwd_depth;      /* sum of backward reach sweeps (scc.cu:1000) */
+  uint32_t trim_iters;     /* sum of trim iterations (scc.cu:1001) */
+  uint32_t wcc_iters;      /* WCC propagation sweeps */
+  uint32_t wcc_step;       /* round in which WCC ran (0 = never) */
+  uint32_t n_trimmed;      /* vertices removed by trim-1 */
+  uint32_t n_trim2;        /* vertices removed by trim-2 */
+  uint32_t n_fb_elim;      /* vertices eliminated as F∩B or trim-2 (reference countElimmed) */
+  uint32_t nscc;           /* number of SCCs */
+  uint32_t largest_scc;    /* size of the largest SCC (0 if not computed) */
+  uint32_t pull_sweeps;    /* reach sweeps done in pull (bottom-up) direction */
+  uint32_t grid_blocks;    /* persistent grid actually launched */
+  uint32_t block_size;
+  uint32_t kernel_launches;/* kernels this call launched */
+  uint32_t reserved;
+  double ms_total;         /* device time of the solve (CUDA events) */
+  double ms_trim;          /* device time by phase (globaltimer inside the persistent kernel) */
+  double ms_fwd;
+  double ms_bwd;
+  double ms_update;
+  double ms_wcc;
+} scc_stats;
+
+/* scc.cu:150 computeSCC(countOfNodes, countOfEdges, nodes, edges, nodesT,
+ * edgesT, alg_opt): the whole decomposition on the bound graph in one
+ * persistent cooperative launch.  labels: host (n+1) or NULL; nscc: count
+ * (reference output "count of SCC"); stats: optional. */
+int scc_solve(scc_ctx *ctx, uint32_t *labels, uint32_t *nscc, scc_stats *stats);
+/* Same, labels left in device memory (d_labels: device (n+1) or NULL). */
+int scc_solve_device(scc_ctx *ctx, uint32_t *d_labels, uint32_t *nscc, scc_stats *stats);
+/* Enqueue the solve on the context stream without synchronising (capturable
+ * in a CUDA graph).  Results: scc_solve_collect after the stream drained. */
+int scc_solve_enqueue(scc_ctx *ctx, uint32_t *d_labels);
+int scc_solve_collect(scc_ctx *ctx, uint32_t *nscc, scc_stats *stats);
+
+/* -------------------------------------------------------- phase level API
+ * Each call runs one phase of the reference driver on the context's device
+ * state (one persistent launch iterating to its device-side fixpoint) and
+ * returns the reference wrapper's return value through the out pointer. */
+/* Reset per-vertex state: nothing eliminated, one partition per segment. */
+int scc_phase_begin(scc_ctx *ctx);
+/* scc_routines.h:47 trim1: global trim-1 to a fixpoint. */
+int scc_trim1(scc_ctx *ctx, uint32_t *iterations);
+/* scc_routines.h:41 trim: partition-aware trim-1 to a fixpoint. */
+int scc_trim(scc_ctx *ctx, uint32_t *iterations);
+/* scc_routines.h:50 trim2: one pass of 2-vertex sink/source SCC removal. */
+int scc_trim2(scc_ctx *ctx, uint32_t *removed);
+/* scc.cu:234-253: pick a pivot for every partition without one (first pivot). */
+int scc_select_pivots(scc_ctx *ctx, uint32_t *n_pivots);
+/* reach_{q,t,d,l}.h fwd_reach[1]_* / bwd_reach[1]_*: dir 0 = forward (out-edges),
+ * 1 = backward (in-edges); variant = SCC_ALG_QUADRATIC/TOPO/DATA/LINEAR/BEST;
+ * first_step != 0 ignores partitions (the *1 variants). depth = sweeps. */
+int scc_reach(scc_ctx *ctx, int dir, int variant, int first_step, uint32_t *depth);
+/* scc_routines.h:33 update: F∩B -> SCC, refine partitions, pick pivots.
+ * has_pivot: 1 if another round is needed. */
+int scc_update(scc_ctx *ctx, int32_t *has_pivot);
+/* scc.cu:42-51 countElimmed: vertices eliminated but not trimmed. */
+int scc_count_elimmed(scc_ctx *ctx, uint32_t *n_elimmed);
+/* scc_routines.h:8 unsetPivots: drop the pivots chosen by the last update. */
+int scc_unset_pivots(scc_ctx *ctx);
+/* wcc.h:23 update_wcc: WCC colouring within partitions, one pivot per colour. */
+int scc_update_wcc(scc_ctx *ctx, uint32_t *depth, int32_t *has_pivot);
+/* Per-vertex state in the reference bit encoding (scc.h:48-93): 1 = B visited,
+ * 2 = F visited, 4 = eliminated, 8 = trimmed, 16 = SCC representative.
+ * states: host (n+1). */
+int scc_get_states(scc_ctx *ctx, uint8_t *states);
+/* Partition id of every active vertex (0 for eliminated ones): host (n+1). */
+int scc_get_ranges(scc_ctx *ctx, uint32_t *ranges);
+/* Finish: canonical labels for all vertices (host n+1) and the SCC count.
+ * Fails with SCC_ERR_STATE while active vertices remain. */
+int scc_get_labels(scc_ctx *ctx, uint32_t *labels, uint32_t *nscc);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GPUSCC_B200_SCC_CAPI_H */
