@@ -1,0 +1,381 @@
+#!/usr/bin/env python
+"""SCC throughput on B200: edges/s and HBM-roofline fraction of the scc_2_w path.
+
+Workload (one step = one complete decomposition): R-MAT, 2^26 vertices,
+2^30 edge samples, (a,b,c,d) = (0.57, 0.19, 0.19, 0.05), vertex ids permuted,
+self-loops dropped, duplicates merged, seed 2, u32 CSR + transpose resident in
+HBM; path = scc_2_w -a h (global trim-1, hybrid reach, WCC colouring and
+trim-2 once, then partition rounds), labels written to device memory.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+value   = m / device time per step (CUDA events on the engine's stream), summed
+          over replicas for N > 1 (a single graph does not shard: N independent
+          replicas, no collective; scaling "weak").
+e2e     = the same metric through the public API from pinned host buffers:
+          each step uploads the CSR (+ device validation), solves and copies
+          the labels back.
+roofline: bytes the decomposition must touch, 2*4(n+1) + 2*4m + 4n (offsets
+          and adjacency of the graph and its transpose once, one u32 label per
+          vertex), divided by the step's device time, against the measured HBM
+          copy bandwidth in MEASURED_PEAKS.json.
+--impl reference: the reference's own CPU decomposition (tarjan.cpp
+          TR_Decomposition, compiled from the reference sources into
+          oracle/_ref) on a bounded sample of the workload, rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+ABC = (0.57, 0.19, 0.19)
+METRIC = "SCC edges/s (R-MAT 2^26 / 2^30 samples, scc_2_w -a h, 1 B200)"
+UNIT = "edges/s"
+
+
+def workload_config(scale: int, samples_log2: int, seed: int, extra: dict | None = None) -> dict:
+    cfg = {
+        "workload": f"rmat{scale}_e{samples_log2}_scc_2_w_hybrid",
+        "graph": f"R-MAT scale {scale}, 2^{samples_log2} samples, (a,b,c,d)=(0.57,0.19,0.19,0.05), "
+                 f"ids permuted, self-loops dropped, duplicates merged, seed {seed}",
+        "path": "scc_2_w -a h: trim-1, hybrid reach (pull-capable topology sweeps, then quadratic), "
+                "WCC + trim-2 once, partition rounds",
+        "index_dtype": "u32",
+        "l2": "inputs larger than L2 (CSR + transpose ~8.6 GB vs 126 MB L2); no flush",
+    }
+    if extra:
+        cfg.update(extra)
+    return cfg
+
+
+def b_alg(n: int, m: int) -> int:
+    return 2 * 4 * (n + 1) + 2 * 4 * m + 4 * n
+
+
+def load_peaks() -> tuple[float, str]:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+        except Exception:
+            pass
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """Polls NVML (read-only) every few ms while the timed region runs."""
+
+    def __init__(self, device_index: int, period_s: float = 0.01):
+        self.dev = device_index
+        self.period = period_s
+        self.samples: list[tuple[float, int, int]] = []
+        self.max_mhz = None
+        self._stop = threading.Event()
+        self._t = None
+        self.ok = False
+
+    def start(self):
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            h = pynvml.nvmlDeviceGetHandleByIndex(self.dev)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM)
+            self._nv, self._h = pynvml, h
+            self.ok = True
+        except Exception:
+            return self
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def _run(self):
+        nv, h = self._nv, self._h
+        while not self._stop.is_set():
+            try:
+                mhz = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                reasons = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                self.samples.append((time.perf_counter(), mhz, reasons))
+            except Exception:
+                pass
+            time.sleep(self.period)
+
+    def stop(self):
+        self._stop.set()
+        if self._t:
+            self._t.join()
+
+    def summary(self, t0: float, t1: float) -> dict:
+        if not self.ok:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvml unavailable"]}
+        win = [s for s in self.samples if t0 <= s[0] <= t1] or self.samples[-3:]
+        names = {
+            0x0000000000000001: "gpu_idle", 0x0000000000000002: "applications_clocks_setting",
+            0x0000000000000004: "sw_power_cap", 0x0000000000000008: "hw_slowdown",
+            0x0000000000000010: "sync_boost", 0x0000000000000020: "sw_thermal_slowdown",
+            0x0000000000000040: "hw_thermal_slowdown", 0x0000000000000080: "hw_power_brake_slowdown",
+            0x0000000000000100: "display_clock_setting",
+        }
+        seen = set()
+        for _, _, r in win:
+            for bit, nm in names.items():
+                if r & bit:
+                    seen.add(nm)
+        return {"sm_mhz": statistics.median([s[1] for s in win]) if win else None, "sm_max_mhz": self.max_mhz,
+                "reasons": sorted(seen), "samples": len(win)}
+
+
+def quiet_stdout():
+    """Redirect fd 1 (the reference's printf) to /dev/null; returns a restore function."""
+    sys.stdout.flush()
+    saved = os.dup(1)
+    dn = os.open(os.devnull, os.O_WRONLY)
+    os.dup2(dn, 1)
+    os.close(dn)
+
+    def restore():
+        sys.stdout.flush()
+        os.dup2(saved, 1)
+        os.close(saved)
+    return restore
+
+
+def cpu_tarjan_rate(scale: int, seed: int, device: int):
+    """Reference Tarjan (oracle/_ref, else the oracle's port) on a R-MAT sample
+    built on the device -> (edges/s, kind, sample description, seconds)."""
+    import numpy as np
+
+    import gpuscc_code_b200 as scc
+    import oracle
+
+    with scc.SCCContext(device) as ctx:
+        ctx.gen_rmat_device(scale, 16 << scale, ABC, seed)
+        g = ctx.download()
+    kind = "reference" if oracle.ref_lib() is not None else "port"
+    restore = quiet_stdout()
+    try:
+        t0 = time.perf_counter()
+        if kind == "reference":
+            cnt, own = oracle.ref_tarjan(g.n, g.nodes, g.edges)
+        else:
+            _, cnt = oracle.tarjan_labels(g.n, g.nodes, g.edges)
+        wall = time.perf_counter() - t0
+    finally:
+        restore()
+    secs = wall
+    sample = (f"R-MAT scale {scale}, 2^{scale + 4} samples, same (a,b,c,d), permuted, seed {seed}: n={g.n}, "
+              f"m={g.m}, {cnt} SCCs; {'tarjan.cpp TR_Decomposition' if kind == 'reference' else 'oracle port'} "
+              f"on 1 host thread, wall {secs:.2f} s")
+    del np
+    return g.m / secs, kind, sample, secs
+
+
+def run_reference(args) -> None:
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import oracle  # noqa: F401
+    import gpuscc_code_b200 as scc
+
+    scale = args.ref_scale
+    with scc.SCCContext(0) as ctx:
+        ctx.gen_rmat_device(scale, 16 << scale, ABC, args.seed)
+        g = ctx.download()
+    kind = "reference" if oracle.ref_lib() is not None else "port"
+    times = []
+    restore = quiet_stdout()
+    try:
+        for i in range(args.warmup + args.steps):
+            t0 = time.perf_counter()
+            if kind == "reference":
+                oracle.ref_tarjan(g.n, g.nodes, g.edges)
+            else:
+                oracle.tarjan_labels(g.n, g.nodes, g.edges)
+            if i >= args.warmup:
+                times.append(time.perf_counter() - t0)
+    finally:
+        restore()
+    per = sum(times) / len(times)
+    value = g.m / per
+    sample = (f"R-MAT scale {scale}, 2^{scale + 4} samples (same generator, (a,b,c,d), permutation, seed "
+              f"{args.seed}): n={g.n}, m={g.m}; one decomposition per step")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": per * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+        "config": workload_config(args.scale, args.samples_log2, args.seed,
+                                  {"reference_sample_scale": scale}),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": kind, "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args) -> None:
+    import numpy as np
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    import gpuscc_code_b200 as scc
+
+    scale, samples = args.scale, 1 << args.samples_log2
+    opts = scc.Options(alg="h", wcc=True, trim2=True)
+    ctx = scc.SCCContext(local, opts)
+    d = ctx.gen_rmat_device(scale, samples, ABC, args.seed)
+    n, m = int(d.n), int(d.m)
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    d_labels = torch.zeros(n + 1, dtype=torch.int32, device=f"cuda:{local}")
+
+    for _ in range(args.warmup):
+        cnt, st = ctx.solve_device(d_labels.data_ptr())
+    nscc_check = cnt
+
+    sampler = ClockSampler(local).start()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t_wall0 = time.perf_counter()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    step_ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+               for _ in range(args.steps)]
+    ev0.record(stream)
+    for i in range(args.steps):
+        step_ev[i][0].record(stream)
+        ctx.solve_enqueue(d_labels.data_ptr())
+        step_ev[i][1].record(stream)
+    ev1.record(stream)
+    cnt, st = ctx.solve_collect()
+    torch.cuda.synchronize()
+    t_wall1 = time.perf_counter()
+    if dist:
+        dist.barrier()
+    sampler.stop()
+    ms = ev0.elapsed_time(ev1)
+    step_ms = [a.elapsed_time(b) for a, b in step_ev]
+    if dist:
+        t = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    if cnt != nscc_check:
+        raise SystemExit(f"SCC count changed between runs: {nscc_check} vs {cnt}")
+    ms_per_step = ms / args.steps
+    value = world * m / (ms_per_step / 1e3)
+    launches = args.steps * 2  # per step: state init + the persistent solve kernel
+
+    # roofline of the dominant kernel (the persistent solve; its init pass is counted with it)
+    peak, peak_kind = load_peaks()
+    kern_ms = statistics.mean(step_ms)
+    achieved = b_alg(n, m) / (kern_ms / 1e3) / 1e9
+    traffic = None
+    prof = ROOT / "profiles" / "traffic_rmat_scc_2_w.json"
+    if prof.exists():
+        try:
+            t = json.loads(prof.read_text())
+            traffic = float(t["bytes_per_edge"]) * m + float(t.get("bytes_per_vertex", 0.0)) * n
+        except Exception:
+            traffic = None
+    clocks = sampler.summary(t_wall0, t_wall1)
+
+    # e2e through the public API from pinned host buffers
+    e2e = None
+    if not args.no_e2e:
+        pin = lambda cnt_: torch.empty(int(cnt_), dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
+        h_nodes, h_edges, h_nodesT, h_edgesT = pin(n + 2), pin(max(m, 1)), pin(n + 2), pin(max(m, 1))
+        ctx.download_into(h_nodes, h_edges, h_nodesT, h_edgesT)
+        hg = scc.HostCSR.from_arrays(h_nodes, h_edges, h_nodesT, h_edgesT, sorted_unique=True)
+        h_labels = pin(n + 1)
+        ctx.upload(hg)  # warm
+        ctx.solve(out=h_labels)
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e2e_steps = max(1, min(args.steps, args.e2e_steps))
+        t0 = time.perf_counter()
+        for _ in range(e2e_steps):
+            ctx.upload(hg)
+            _, c2, _ = ctx.solve(out=h_labels)
+        torch.cuda.synchronize()
+        e2e_s = (time.perf_counter() - t0) / e2e_steps
+        if dist:
+            t = torch.tensor([e2e_s], dtype=torch.float64, device=f"cuda:{local}")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_s = float(t.item())
+        if c2 != cnt:
+            raise SystemExit("e2e SCC count differs from the device-resident run")
+        e2e = {"value": world * m / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 2 * 4 * (n + 2) + 2 * 4 * m,
+               "d2h_bytes_per_step": 4 * (n + 1), "ms_per_step": e2e_s * 1e3, "steps": e2e_steps}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        rate, kind, sample, _ = cpu_tarjan_rate(args.cpu_scale, args.seed, local)
+        cpu = {"value": rate, "unit": UNIT, "cores": 1, "kind": kind, "sample": sample,
+               "host_cores_available": os.cpu_count()}
+
+    if dist:
+        dist.destroy_process_group()
+    if rank != 0:
+        ctx.close()
+        return
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u32", "data": "synthetic (R-MAT generated on the device, seed 2)",
+        "config": workload_config(scale, args.samples_log2, args.seed,
+                                  {"n": n, "m": m, "nscc": cnt, "parallelism": f"replicas{world}"}),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                     "kernel": "scc_persistent<256> (+ per-step init pass)", "kernel_ms": kern_ms,
+                     "algorithmic_bytes": b_alg(n, m)},
+        "clocks": clocks,
+        "gpu_launches": launches,
+        "e2e": e2e,
+        "cpu_baseline": cpu,
+        "stats": {k: (round(v, 4) if isinstance(v, float) else v) for k, v in st.items()},
+    }
+    print(json.dumps(line), flush=True)
+    ctx.close()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--scale", type=int, default=26)
+    ap.add_argument("--samples-log2", type=int, default=30)
+    ap.add_argument("--seed", type=int, default=2)
+    ap.add_argument("--cpu-scale", type=int, default=24, help="R-MAT scale of the cpu_baseline sample")
+    ap.add_argument("--ref-scale", type=int, default=23, help="R-MAT scale of each --impl reference step")
+    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,7 +1,7 @@
 """ctypes binding of include/scc_capi.h (libgpuscc_b200.so, built in-tree).
 
 There is no fallback: if the shared library is missing or fails to load,
-importing this module raises.  Build it with `python -m gpuscc_code_b200.build`.
+importing this module raises.  Build it with `python gpuscc_code_b200/build.py`.
 """
 from __future__ import annotations
 
@@ -91,6 +91,7 @@ SIGNATURES = [
     ("scc_ctx_upload", C.c_int, [C.c_void_p, C.POINTER(scc_host_csr)]),
     ("scc_ctx_bind_device", C.c_int, [C.c_void_p, C.POINTER(scc_dev_csr)]),
     ("scc_ctx_download", C.c_int, [C.c_void_p, C.POINTER(scc_host_csr)]),
+    ("scc_ctx_download_into", C.c_int, [C.c_void_p, u32p, u32p, u32p, u32p]),
     ("scc_ctx_set_segments", C.c_int, [C.c_void_p, C.c_uint32, u32p]),
     ("scc_solve", C.c_int, [C.c_void_p, u32p, u32p, C.POINTER(scc_stats)]),
     ("scc_solve_device", C.c_int, [C.c_void_p, C.c_void_p, u32p, C.POINTER(scc_stats)]),
@@ -120,7 +121,7 @@ class SCCError(RuntimeError):
 
 def _load() -> C.CDLL:
     if not LIB_PATH.exists():
-        raise ImportError(f"{LIB_PATH} is not built; run `python -m gpuscc_code_b200.build`")
+        raise ImportError(f"{LIB_PATH} is not built; run `python gpuscc_code_b200/build.py`")
     lib = C.CDLL(str(LIB_PATH))
     for name, res, args in SIGNATURES:
         fn = getattr(lib, name)

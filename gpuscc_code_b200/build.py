@@ -3,7 +3,7 @@
 CUDA sources are compiled for sm_100a only (`-gencode arch=compute_100a,code=sm_100a`),
 host sources with g++; objects go to gpuscc_code_b200/_build, the shared
 library next to this file and the apps to gpuscc_code_b200/bin.
-Run `python -m gpuscc_code_b200.build [--force]`.
+Run `python gpuscc_code_b200/build.py [--force]` (by path: importing the package loads the library).
 """
 from __future__ import annotations
 

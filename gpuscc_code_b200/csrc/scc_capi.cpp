@@ -377,16 +377,6 @@ int scc_ctx_upload(scc_ctx *c, const scc_host_csr *g) {
   if (g->nodes[g->n + 1] != g->m || g->nodesT[g->n + 1] != g->m)
     return set_error(SCC_ERR_INVALID, "nodes[n+1] (%u) / nodesT[n+1] (%u) differ from m (%u)", g->nodes[g->n + 1],
                      g->nodesT[g->n + 1], g->m);
-  // the kernels trust the layout: reject anything that would index outside it
-  for (int t = 0; t < 2; ++t) {
-    const uint32_t *o = t ? g->nodesT : g->nodes, *a = t ? g->edgesT : g->edges;
-    if (g->n && o[1] != 0) return set_error(SCC_ERR_INVALID, "%s[1] must be 0", t ? "nodesT" : "nodes");
-    for (uint32_t v = 1; v <= g->n; ++v)
-      if (o[v] > o[v + 1]) return set_error(SCC_ERR_INVALID, "%s decreases at vertex %u", t ? "nodesT" : "nodes", v);
-    for (uint32_t i = 0; i < g->m; ++i)
-      if (a[i] < 1 || a[i] > g->n)
-        return set_error(SCC_ERR_INVALID, "%s[%u] = %u is outside 1..%u", t ? "edgesT" : "edges", i, a[i], g->n);
-  }
   int rc = use_device(c);
   if (rc) return rc;
   const size_t ob = ((size_t)g->n + 2) * 4, eb = ((size_t)g->m + 1) * 4;
@@ -408,12 +398,24 @@ int scc_ctx_upload(scc_ctx *c, const scc_host_csr *g) {
     c->d_offT = c->g_offT.as<uint32_t>();
     c->d_adjT = c->g_adjT.as<uint32_t>();
   }
+  // the kernels trust the layout: reject anything that would index outside it
+  CK(c->ctl.ensure(sizeof(sccb::Ctl)), "alloc control block");
+  for (int t = 0; t < 2; ++t) {
+    uint32_t bad = 0;
+    CK(sccb::check_device_csr(t ? c->d_offT : c->d_off, t ? c->d_adjT : c->d_adj, g->n, g->m, c->ctl.as<uint32_t>(),
+                              &bad, c->stream),
+       "CSR check");
+    if (bad) {
+      c->have_graph = false;
+      return set_error(SCC_ERR_INVALID, "%s: %s", t ? "transpose" : "graph",
+                       (bad & 1u) ? "offsets are not monotone from 0 to m" : "a neighbour id is outside 1..n");
+    }
+  }
   c->n = g->n;
   c->m = g->m;
   c->sorted_unique = g->sorted_unique;
   c->have_graph = true;
   c->phase_ready = false;
-  CK(cudaStreamSynchronize(c->stream), "upload");
   return ensure_state(c);
 }
 
@@ -525,6 +527,26 @@ int scc_ctx_download(scc_ctx *c, scc_host_csr *out) {
   return SCC_OK;
 }
 
+int scc_ctx_download_into(scc_ctx *c, uint32_t *nodes, uint32_t *edges, uint32_t *nodesT, uint32_t *edgesT) {
+  sccb::clear_error();
+  int rc = need_graph(c);
+  if (rc) return rc;
+  if (!nodes || !nodesT || (c->m && (!edges || !edgesT))) return set_error(SCC_ERR_INVALID, "null output");
+  rc = use_device(c);
+  if (rc) return rc;
+  const size_t ob = ((size_t)c->n + 2) * 4, eb = (size_t)c->m * 4;
+  CK(cudaMemcpyAsync(nodes, c->d_off, ob, cudaMemcpyDeviceToHost, c->stream), "download");
+  CK(cudaMemcpyAsync(nodesT, c->d_offT, ob, cudaMemcpyDeviceToHost, c->stream), "download");
+  if (eb) {
+    CK(cudaMemcpyAsync(edges, c->d_adj, eb, cudaMemcpyDeviceToHost, c->stream), "download");
+    CK(cudaMemcpyAsync(edgesT, c->d_adjT, eb, cudaMemcpyDeviceToHost, c->stream), "download");
+  }
+  CK(cudaStreamSynchronize(c->stream), "download");
+  nodes[0] = 0;
+  nodesT[0] = 0;
+  return SCC_OK;
+}
+
 int scc_ctx_set_segments(scc_ctx *c, uint32_t nseg, const uint32_t *seg_first) {
   sccb::clear_error();
   if (!c) return set_error(SCC_ERR_INVALID, "null context");
@@ -556,7 +578,7 @@ int scc_solve_enqueue(scc_ctx *c, uint32_t *d_labels) {
   c->launches = 0;
   rc = reset_state(c);
   if (rc) return rc;
-  CK(cudaEventRecord(c->ev0, c->stream), "event");
+  CK(cudaEventRecord(c->ev0, c->stream), "event");  // ms_total: the persistent kernel alone
   rc = launch(c, sccb::PH_SOLVE, 0, 0, 0, d_labels);
   if (rc) return rc;
   CK(cudaEventRecord(c->ev1, c->stream), "event");

@@ -79,9 +79,14 @@ class HostCSR:
 
     @classmethod
     def from_arrays(cls, nodes, edges, nodesT, edgesT, sorted_unique: bool = False) -> "HostCSR":
+        """Wraps caller arrays without copying when they already are contiguous
+        uint32 (e.g. pinned buffers); edges/edgesT need at least m entries."""
         nodes, nodesT = _u32(nodes), _u32(nodesT)
-        edges = _u32(np.append(np.asarray(edges, dtype=np.uint32), np.uint32(0)))
-        edgesT = _u32(np.append(np.asarray(edgesT, dtype=np.uint32), np.uint32(0)))
+        edges, edgesT = _u32(edges), _u32(edgesT)
+        if len(edges) == 0:
+            edges = np.zeros(1, np.uint32)
+        if len(edgesT) == 0:
+            edgesT = np.zeros(1, np.uint32)
         n = len(nodes) - 2
         raw = scc_host_csr(n=n, m=int(nodes[n + 1]), nnz_header=int(nodes[n + 1]), symmetric=0,
                            sorted_unique=int(sorted_unique), owned=0, nodes=_ptr(nodes), edges=_ptr(edges),
@@ -245,9 +250,18 @@ class SCCContext:
         check(lib.scc_ctx_set_segments(self._h, len(s) - 1, _ptr(s)))
 
     # -------------------------------------------------------------- solve
-    def solve(self, want_labels: bool = True):
-        """scc.cu:150 computeSCC -> (labels[n+1] or None, count, stats dict)."""
-        labels = np.zeros(self.n + 1, dtype=np.uint32) if want_labels else None
+    def download_into(self, nodes: np.ndarray, edges: np.ndarray, nodesT: np.ndarray, edgesT: np.ndarray):
+        """Copy the bound graph into caller-owned uint32 host arrays (n+2 / m)."""
+        check(lib.scc_ctx_download_into(self._h, _ptr(nodes), _ptr(edges), _ptr(nodesT), _ptr(edgesT)))
+
+    def solve(self, want_labels: bool = True, out: np.ndarray | None = None):
+        """scc.cu:150 computeSCC -> (labels[n+1] or None, count, stats dict).
+        `out`: optional caller-owned uint32 array of n+1 entries for the labels."""
+        if out is not None:
+            labels = out
+        else:
+            labels = np.zeros(self.n + 1, dtype=np.uint32) if want_labels else None
+        want_labels = labels is not None
         cnt = C.c_uint32()
         st = scc_stats()
         check(lib.scc_solve(self._h, _ptr(labels) if want_labels else None, C.byref(cnt), C.byref(st)))

@@ -165,6 +165,9 @@ int scc_ctx_upload(scc_ctx *ctx, const scc_host_csr *csr);
 int scc_ctx_bind_device(scc_ctx *ctx, const scc_dev_csr *csr);
 /* Copy the bound graph back to the host (for the apps' -t and for tests). */
 int scc_ctx_download(scc_ctx *ctx, scc_host_csr *out);
+/* Same, into caller-owned host arrays (nodes/nodesT: n+2, edges/edgesT: m),
+ * e.g. pinned buffers for later uploads. */
+int scc_ctx_download_into(scc_ctx *ctx, uint32_t *nodes, uint32_t *edges, uint32_t *nodesT, uint32_t *edgesT);
 /* Independent graphs packed in one CSR (batching): segment s owns vertices
  * seg_first[s] .. seg_first[s+1]-1 (1-based, seg_first[0] = 1,
  * seg_first[nseg] = n+1; no edge may cross segments).  nseg = 0 clears. */
