@@ -95,6 +95,7 @@ SIGNATURES = [
     ("scc_ctx_set_segments", C.c_int, [C.c_void_p, C.c_uint32, u32p]),
     ("scc_solve", C.c_int, [C.c_void_p, u32p, u32p, C.POINTER(scc_stats)]),
     ("scc_solve_device", C.c_int, [C.c_void_p, C.c_void_p, u32p, C.POINTER(scc_stats)]),
+    ("scc_solve_noalloc", C.c_int, [C.POINTER(scc_dev_csr), C.POINTER(scc_opts), C.c_void_p, u32p, C.c_void_p]),
     ("scc_solve_enqueue", C.c_int, [C.c_void_p, C.c_void_p]),
     ("scc_solve_collect", C.c_int, [C.c_void_p, u32p, C.POINTER(scc_stats)]),
     ("scc_phase_begin", C.c_int, [C.c_void_p]),

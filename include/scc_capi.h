@@ -205,6 +205,20 @@ typedef struct scc_stats {
 int scc_solve(scc_ctx *ctx, uint32_t *labels, uint32_t *nscc, scc_stats *stats);
 /* Same, labels left in device memory (d_labels: device (n+1) or NULL). */
 int scc_solve_device(scc_ctx *ctx, uint32_t *d_labels, uint32_t *nscc, scc_stats *stats);
+/* No counterpart in the reference (it cudaMallocs everything per call).
+ * The whole decomposition for callers that cannot allocate device memory —
+ * code running while a stream is captured, plugins whose host framework owns
+ * the whole device-memory budget, latency-critical loops that must not hit
+ * the allocator's implicit synchronisation.  Needs no context: all scratch
+ * lives in one static device array (about 4.7 MB per GPU, held until the
+ * process exits), so graphs are limited to 65536 vertices and 4194304 edges
+ * (SCC_ERR_CAPACITY beyond).  g: device CSR in the reference layout;
+ * d_labels: device (n+1) output or NULL; stream: cudaStream_t or NULL.
+ * Calls that overlap on the GPU share the array and race; serialise them.
+ * The first call on each device does a one-time set-up for that device, so
+ * make it before any stream capture. */
+int scc_solve_noalloc(const scc_dev_csr *g, const scc_opts *opts, uint32_t *d_labels, uint32_t *nscc,
+                      void *stream);
 /* Enqueue the solve on the context stream without synchronising (capturable
  * in a CUDA graph).  Results: scc_solve_collect after the stream drained. */
 int scc_solve_enqueue(scc_ctx *ctx, uint32_t *d_labels);
