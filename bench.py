@@ -263,6 +263,8 @@ def run_ours(args) -> None:
         step_ev[i][1].record(stream)
     ev1.record(stream)
     cnt, st = ctx.solve_collect()
+    prof_last = ctx.profile()  # device phase timers of the last timed step
+    trace_last = ctx.trace()
     torch.cuda.synchronize()
     t_wall1 = time.perf_counter()
     if dist:
@@ -349,6 +351,8 @@ def run_ours(args) -> None:
         "e2e": e2e,
         "cpu_baseline": cpu,
         "stats": {k: (round(v, 4) if isinstance(v, float) else v) for k, v in st.items()},
+        "profile_ms": {k: v for k, v in prof_last.items()},
+        "trace": trace_last if args.trace else None,
     }
     print(json.dumps(line), flush=True)
     ctx.close()
@@ -368,6 +372,7 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--trace", action="store_true", help="include the per-sweep device trace in the line")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

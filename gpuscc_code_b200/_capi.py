@@ -35,6 +35,7 @@ class scc_opts(C.Structure):
         ("switch_permille", C.c_int32), ("trim_depth", C.c_int32), ("pull_alpha", C.c_int32),
         ("pull_beta", C.c_int32), ("warp_degree", C.c_uint32), ("heavy_degree", C.c_uint32),
         ("max_iters", C.c_uint32), ("grid_blocks", C.c_uint32), ("timeout_ms", C.c_uint32),
+        ("trim_first_depth", C.c_int32),
     ]
 
 
@@ -98,6 +99,8 @@ SIGNATURES = [
     ("scc_solve_noalloc", C.c_int, [C.POINTER(scc_dev_csr), C.POINTER(scc_opts), C.c_void_p, u32p, C.c_void_p]),
     ("scc_solve_enqueue", C.c_int, [C.c_void_p, C.c_void_p]),
     ("scc_solve_collect", C.c_int, [C.c_void_p, u32p, C.POINTER(scc_stats)]),
+    ("scc_get_profile", C.c_int, [C.c_void_p, C.POINTER(C.c_double), u32p]),
+    ("scc_get_trace", C.c_int, [C.c_void_p, u32p, u32p, u32p, u32p, C.POINTER(C.c_double)]),
     ("scc_phase_begin", C.c_int, [C.c_void_p]),
     ("scc_trim1", C.c_int, [C.c_void_p, u32p]),
     ("scc_trim", C.c_int, [C.c_void_p, u32p]),

@@ -120,7 +120,7 @@ int ensure_state(scc_ctx *c) {
   const uint32_t cn = n > c->cap_n ? n : c->cap_n;
   const uint32_t ch = hcap > c->cap_h ? hcap : c->cap_h;
   const size_t vb = ((size_t)cn + 1) * 4;
-  const uint32_t nw = ((((uint32_t)(((uint64_t)cn + 1 + 31) / 32)) + 3u) & ~3u) + 4u;
+  const uint32_t nw = sccb::bitmap_words(cn) + sccb::kBitmapSlack;
   CK(c->label.ensure(vb), "alloc labels");
   CK(c->range.ensure(vb), "alloc ranges");
   CK(c->rpivot.ensure(vb), "alloc pivots");
@@ -163,7 +163,7 @@ sccb::Params make_params(scc_ctx *c, uint32_t *out_labels) {
   s.rpivot = c->rpivot.as<uint32_t>();
   s.aux = c->aux.as<uint32_t>();
   // bitmaps sized for this graph (words beyond it are never touched)
-  const uint32_t nw = ((((uint32_t)(((uint64_t)c->n + 1 + 31) / 32)) + 3u) & ~3u);
+  const uint32_t nw = sccb::bitmap_words(c->n);
   uint32_t *bm = c->bitmaps.as<uint32_t>();
   const uint32_t stride = c->nwords;
   s.elim = bm + 0 * (size_t)stride;
@@ -208,6 +208,9 @@ sccb::Params make_params(scc_ctx *c, uint32_t *out_labels) {
   e.heavy_degree = o.heavy_degree ? o.heavy_degree : 4096u;
   e.max_iters = o.max_iters ? o.max_iters : (1u << 20);
   e.timeout_ns = (unsigned long long)(o.timeout_ms ? o.timeout_ms : 10000u) * 1000000ull;
+  e.trim_first_depth = o.trim_first_depth;
+  // labels are written straight into the caller's device buffer when given
+  if (out_labels) s.label = out_labels;
   return p;
 }
 
@@ -303,6 +306,7 @@ void scc_opts_default(scc_opts *o) {
   o->trim_depth = 0;
   o->pull_alpha = 0;
   o->pull_beta = 0;
+  o->trim_first_depth = 1;
 }
 
 int scc_ctx_create(int device, const scc_opts *opts, scc_ctx **out) {
@@ -326,6 +330,7 @@ int scc_ctx_create(int device, const scc_opts *opts, scc_ctx **out) {
   cudaError_t e = cudaSetDevice(device);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaMallocHost((void **)&c->h_ctl, sizeof(sccb::Ctl));
+  if (e == cudaSuccess) std::memset(c->h_ctl, 0, sizeof(sccb::Ctl));
   if (e == cudaSuccess) e = cudaEventCreate(&c->ev0);
   if (e == cudaSuccess) e = cudaEventCreate(&c->ev1);
   if (e != cudaSuccess) {
@@ -613,6 +618,30 @@ int scc_solve(scc_ctx *c, uint32_t *labels, uint32_t *nscc, scc_stats *st) {
     CK(cudaMemcpyAsync(labels, c->label.p, ((size_t)c->n + 1) * 4, cudaMemcpyDeviceToHost, c->stream), "labels D2H");
     CK(cudaStreamSynchronize(c->stream), "labels D2H");
     labels[0] = 0;
+  }
+  return SCC_OK;
+}
+
+int scc_get_profile(scc_ctx *c, double *ms, uint32_t *counts) {
+  sccb::clear_error();
+  if (!c) return set_error(SCC_ERR_INVALID, "null context");
+  for (int i = 0; i < 16; ++i) {
+    if (ms) ms[i] = c->h_ctl->prof_ns[i] * 1e-6;
+    if (counts) counts[i] = c->h_ctl->prof_cnt[i];
+  }
+  return SCC_OK;
+}
+
+int scc_get_trace(scc_ctx *c, uint32_t *n, uint32_t *slot, uint32_t *a, uint32_t *b, double *ms) {
+  sccb::clear_error();
+  if (!c || !n) return set_error(SCC_ERR_INVALID, "null argument");
+  const uint32_t cnt = c->h_ctl->trace_n < sccb::kTrace ? c->h_ctl->trace_n : sccb::kTrace;
+  *n = cnt;
+  for (uint32_t i = 0; i < cnt; ++i) {
+    if (slot) slot[i] = c->h_ctl->trace_slot[i];
+    if (a) a[i] = c->h_ctl->trace_a[i];
+    if (b) b[i] = c->h_ctl->trace_b[i];
+    if (ms) ms[i] = c->h_ctl->trace_ns[i] * 1e-6;
   }
   return SCC_OK;
 }

@@ -62,6 +62,40 @@ struct Eng {
   __device__ uint32_t *err() { return &c->gs.err; }
   __device__ void fail(uint32_t bits) { atomicOr(&c->gs.err, bits); }
   __device__ bool is_lead() { return blockIdx.x == 0 && threadIdx.x == 0; }
+  // CTA 0 / thread 0 accumulates the time since t0 under profile slot `slot`
+  __device__ void prof(uint32_t slot, unsigned long long t0, uint32_t a = 0, uint32_t b = 0) {
+    if (is_lead()) {
+      const unsigned long long dt = globaltimer_ns() - t0;
+      c->prof_ns[slot] += dt;
+      c->prof_cnt[slot] += 1;
+      const uint32_t i = c->trace_n;
+      if (i < kTrace) {
+        c->trace_slot[i] = slot;
+        c->trace_a[i] = a;
+        c->trace_b[i] = b;
+        c->trace_ns[i] = dt;
+        c->trace_n = i + 1;
+      }
+    }
+  }
+
+  // Sets bit v of `bm` for every lane with pred; all 32 lanes must call.
+  // Lanes whose ids share a bitmap word combine into one atomicOr instead of
+  // 32 serialised ones.  aligned: lane i holds id 32*w + i of a single word w
+  // (full-mode for_vertices), so one ballot forms the word.
+  __device__ void warp_set_bits(uint32_t *bm, uint32_t v, bool pred, bool aligned) {
+    if (aligned) {
+      const uint32_t bits = __ballot_sync(kFull, pred);
+      if (bits && lane_id() == 0) atomicOr(bm + (v >> 5), bits);
+      return;
+    }
+    const uint32_t word = pred ? (v >> 5) : kNone;
+    const uint32_t grp = __match_any_sync(kFull, word);
+    if (pred) {
+      const uint32_t bits = __reduce_or_sync(grp, 1u << (v & 31u));
+      if (lane_id() == (uint32_t)(__ffs(grp) - 1)) atomicOr(bm + word, bits);
+    }
+  }
 
   // block-reduced atomicAdd into a global counter
   __device__ void add_count(uint32_t *dst, uint32_t x) {
@@ -75,23 +109,74 @@ struct Eng {
   __device__ uint32_t nwarps() const { return (gridDim.x * BS) >> 5; }
 
   // Calls f(v, valid) for every vertex of the current sweep set, all 32
-  // lanes of a warp together (valid = false pads the last warp).  Full mode
-  // covers ids 0 .. nwords*32-1 so that a warp owns exactly one bitmap word.
-  template <class F>
-  __device__ void for_vertices(F &&f) {
+  // lanes of a warp together (valid = false pads the last block), then
+  // after() once per iteration with the whole CTA (every CTA runs whole
+  // iterations, so after() may __syncthreads).  Full mode covers ids
+  // 0 .. nwords*32-1 so that a warp owns exactly one bitmap word.
+  template <class F, class H>
+  __device__ void for_vertices(F &&f, H &&after) {
     if (list_mode) {
       const uint32_t *lst = P.s.act[act_sel];
       const uint32_t cnt = act_count;
-      const uint32_t lim = (cnt + 31u) & ~31u;
-      for (uint32_t i = gtid(); i < lim; i += gstride()) {
+      const uint32_t lim = (cnt + BS - 1u) / BS * BS;
+      for (uint32_t base = blockIdx.x * BS; base < lim; base += gstride()) {
+        const uint32_t i = base + threadIdx.x;
         const bool valid = i < cnt;
         f(valid ? ldm(lst + i) : 0u, valid);
+        after();
       }
     } else {
-      const uint32_t lim = P.s.nwords * 32u;
+      const uint32_t lim = P.s.nwords * 32u;  // a multiple of 1024 >= BS
       const uint32_t n = P.g.n;
-      for (uint32_t v = gtid(); v < lim; v += gstride()) f(v, v >= 1 && v <= n);
+      for (uint32_t base = blockIdx.x * BS; base < lim; base += gstride()) {
+        const uint32_t v = base + threadIdx.x;
+        f(v, v >= 1 && v <= n);
+        after();
+      }
     }
+  }
+  template <class F>
+  __device__ void for_vertices(F &&f) {
+    for_vertices(f, [] {});
+  }
+
+  // Warp-staged worklist append.  Items a warp emits during a sweep collect
+  // in its own shared-memory segment and reach the global list kStage at a
+  // time with one atomicAdd, so a sweep that emits millions of items does not
+  // serialise every warp of the grid on one counter word in L2, and no CTA
+  // barrier is involved (warps never wait for each other).
+  struct Stage {
+    uint32_t *dst;
+    uint32_t *count;
+    uint32_t cap;
+    uint32_t n;  // items staged by this warp (identical in all 32 lanes)
+  };
+  static constexpr uint32_t kStage = 256;
+  __device__ uint32_t *stage_buf() {
+    __shared__ uint32_t buf[BS / 32][kStage];
+    return buf[threadIdx.x >> 5];
+  }
+  __device__ void stage_flush(Stage &q) {
+    __syncwarp();
+    uint32_t base = 0;
+    if (lane_id() == 0 && q.n) base = atomicAdd(q.count, q.n);
+    base = __shfl_sync(kFull, base, 0);
+    const uint32_t *buf = stage_buf();
+    for (uint32_t i = lane_id(); i < q.n; i += 32) {
+      const uint32_t pos = base + i;
+      if (pos < q.cap) q.dst[pos] = buf[i];
+      else atomicOr(err(), kErrQueueOverflow);
+    }
+    q.n = 0;
+    __syncwarp();
+  }
+  // all 32 lanes of the warp call it together
+  __device__ void stage_put(Stage &q, bool pred, uint32_t v) {
+    const uint32_t mask = __ballot_sync(kFull, pred);
+    if (!mask) return;
+    if (pred) stage_buf()[q.n + __popc(mask & lanemask_lt())] = v;
+    q.n += __popc(mask);
+    if (q.n > kStage - 32) stage_flush(q);
   }
   // every id 0 .. nwords*32-1 regardless of the active list
   template <class F>
@@ -100,10 +185,10 @@ struct Eng {
     const uint32_t n = P.g.n;
     for (uint32_t v = gtid(); v < lim; v += gstride()) f(v, v >= 1 && v <= n);
   }
-  // grid-stride over [0, cnt), whole warps
+  // grid-stride over [0, cnt), whole CTAs
   template <class F>
   __device__ void for_items(uint32_t cnt, F &&f) {
-    const uint32_t lim = (cnt + 31u) & ~31u;
+    const uint32_t lim = (cnt + BS - 1u) / BS * BS;
     for (uint32_t i = gtid(); i < lim; i += gstride()) f(i, i < cnt);
   }
 
@@ -138,31 +223,59 @@ struct Eng {
     return false;
   }
 
-  __device__ void mark_trimmed(uint32_t v) {
-    P.s.label[v] = v;
-    bit_set(P.s.tflag, v);
-    bit_set(P.s.elim, v);
-  }
-
   // Returns the number of trim iterations.  Iteration 1 sweeps the active
   // set; later iterations only re-check neighbours of vertices trimmed in the
   // previous one (deduplicated through the `queued` bitmap).
-  __device__ uint32_t trim(bool ranged, bool snap, uint32_t max_it) {
+  // pick: also elect the first pivot among the survivors of the sweep (only
+  // valid when no further trim iteration follows, i.e. max_it == 1).
+  __device__ uint32_t trim(bool ranged, bool snap, uint32_t max_it, bool pick = false) {
     const EngState &s = P.s;
     const EngGraph &g = P.g;
+    unsigned long long t0 = globaltimer_ns();
     uint32_t ntrim = 0;
+    unsigned long long best = ~0ull;
+    Stage tq{s.qa, cur() + C_Q, s.qcap, 0};
     for_vertices([&](uint32_t v, bool valid) {
+      const uint32_t ew = ldm(s.elim + (v >> 5));
+      if (!list_mode && ~ew == 0u) return;  // whole word already eliminated
+      const uint32_t vv = valid ? v : 0u;
+      const bool lv = valid && !((ew >> (v & 31u)) & 1u);
+      // all four offsets are requested before anything depends on them
+      const uint32_t a0 = ldg(g.off + vv), a1 = ldg(g.off + vv + 1);
+      const uint32_t b0 = ldg(g.offT + vv), b1 = ldg(g.offT + vv + 1);
       bool t = false;
-      if (valid && live(v)) {
-        const uint32_t rv = ranged ? ldm(s.range + v) : 0u;
-        t = !live_nbr(g.off, g.adj, v, rv, ranged, snap) || !live_nbr(g.offT, g.adjT, v, rv, ranged, snap);
-        if (t) mark_trimmed(v);
+      if (lv) {
+        if (snap) {  // nothing eliminated yet, lists sorted-unique: degrees decide
+          const uint32_t dout = a1 - a0, din = b1 - b0;
+          const uint32_t x = dout == 1 ? ldg(g.adj + a0) : 0u;
+          const uint32_t y = din == 1 ? ldg(g.adjT + b0) : 0u;
+          t = !(dout >= 2 || (dout == 1 && x != v)) || !(din >= 2 || (din == 1 && y != v));
+        } else {
+          const uint32_t rv = ranged ? ldm(s.range + v) : 0u;
+          t = !live_nbr(g.off, g.adj, v, rv, ranged, false) || !live_nbr(g.offT, g.adjT, v, rv, ranged, false);
+        }
+        if (t) s.label[v] = v;
+        if (pick && !t) {
+          const unsigned long long key = ((unsigned long long)prio(v) << 32) | v;
+          best = key < best ? key : best;
+        }
       }
-      warp_push(s.qa, cur() + C_Q, s.qcap, v, t, err());
+      // neighbours can only lose their last partner if v has edges at all
+      const bool q = t && (a1 != a0 || b1 != b0);
+      warp_set_bits(s.tflag, v, t, !list_mode);
+      warp_set_bits(s.elim, v, t, !list_mode);
+      stage_put(tq, q, v);
       ntrim += t;
     });
+    stage_flush(tq);
     add_count(&c->n_trimmed, ntrim);
+    if (pick) {
+      best = block_min_u64(best);
+      if (threadIdx.x == 0 && best != ~0ull) atomicMin(&c->best, best);
+    }
     if (!bar(100)) return 1;
+    prof(PR_TRIM_SWEEP, t0, rdprv(C_Q));
+    t0 = globaltimer_ns();
     uint32_t it = 1;
     uint32_t nq = rdprv(C_Q);
     while (nq > 0 && it < max_it) {
@@ -193,9 +306,11 @@ struct Eng {
           if (live(u)) {
             const uint32_t ru = ranged ? ldm(s.range + u) : 0u;
             t = !live_nbr(g.off, g.adj, u, ru, ranged, false) || !live_nbr(g.offT, g.adjT, u, ru, ranged, false);
-            if (t) mark_trimmed(u);
+            if (t) s.label[u] = u;
           }
         }
+        warp_set_bits(s.tflag, u, t, false);
+        warp_set_bits(s.elim, u, t, false);
         warp_push(s.qa, cur() + C_Q, s.qcap, u, t, err());
         ntrim += t;
       });
@@ -204,6 +319,7 @@ struct Eng {
       nq = rdprv(C_Q);
       ++it;
     }
+    if (it > 1) prof(PR_TRIM_WL, t0, it - 1);
     return it;
   }
 
@@ -222,6 +338,10 @@ struct Eng {
     best = block_min_u64(best);
     if (threadIdx.x == 0 && best != ~0ull) atomicMin(&c->best, best);
     if (!bar(200)) return 0;
+    return commit_first_pivot();
+  }
+  // c->best holds the elected (priority, id) key; make it the pivot
+  __device__ uint32_t commit_first_pivot() {
     const unsigned long long b = ldm64(&c->best);
     const uint32_t p = b == ~0ull ? 0u : (uint32_t)b;
     // c->best is reset by the lead after the next barrier (everyone has read it by then)
@@ -253,23 +373,30 @@ struct Eng {
       s_val[i] = ~0ull;
     }
     __syncthreads();
-    uint32_t nelim = 0;
+    uint32_t nelim = 0, nfound = 0;
     // A: eliminate F∩B, elect pivots (CTA-local min per key, flushed below)
     for_vertices([&](uint32_t v, bool valid) {
+      const uint32_t w = v >> 5;
+      const uint32_t ew = ldm(s.elim + w), fw = ldm(s.fvis + w), bw = ldm(s.bvis + w);
+      if (!list_mode && ~ew == 0u) return;  // whole word already eliminated
+      const uint32_t r = ldm(s.range + (valid ? v : 0u));
       uint32_t key = kNone;
       unsigned long long val = ~0ull;
-      if (valid && live(v)) {
-        const bool f = bit_test(s.fvis, v), b = bit_test(s.bvis, v);
-        const uint32_t r = ldm(s.range + v);
+      bool fb = false;
+      if (valid && !((ew >> (v & 31u)) & 1u)) {
+        const bool f = (fw >> (v & 31u)) & 1u, b = (bw >> (v & 31u)) & 1u;
         if (f && b) {
-          s.label[v] = ldm(s.rpivot + r);
-          bit_set(s.elim, v);
+          const uint32_t p = ldm(s.rpivot + r);
+          s.label[v] = p;
+          fb = true;
           ++nelim;
+          nfound += p == v;  // one SCC per eliminated pivot
         } else {
           key = 3u * r + (f ? 1u : 0u) + (b ? 2u : 0u);
           val = ((unsigned long long)prio(v) << 32) | v;
         }
       }
+      warp_set_bits(s.elim, v, fb, !list_mode);
       const uint32_t grp = __match_any_sync(kFull, key);
       if (key != kNone) {
         const uint32_t hi = (uint32_t)(val >> 32), lo = (uint32_t)val;
@@ -294,6 +421,7 @@ struct Eng {
       if (key != kNone && ldm64(s.slot + key) > s_val[i]) atomicMin(s.slot + key, s_val[i]);
     }
     add_count(&c->n_fbe, nelim);
+    add_count(&c->n_fbscc, nfound);
     if (!bar(300)) return;
     // B: new partition id = elected pivot; pivots go to the pivot list
     __shared__ unsigned long long s_hit[kSlotCache];  // (key << 32) | pivot
@@ -375,10 +503,63 @@ struct Eng {
   // current direction when it is live, in the source's partition (unless
   // first step) and not visited yet; exactly one caller wins the claim.
   __device__ bool try_visit(uint32_t *vis, uint32_t u, bool ranged, uint32_t rsrc) {
-    if (bit_test(vis, u)) return false;
-    if (!live(u)) return false;
+    const uint32_t w = u >> 5, b = 1u << (u & 31u);
+    const uint32_t vw = ldm(vis + w);        // both bitmap words are requested
+    const uint32_t ew = ldm(P.s.elim + w);   // before either is tested
+    if ((vw | ew) & b) return false;
     if (ranged && ldm(P.s.range + u) != rsrc) return false;
-    return bit_claim(vis, u);
+    return !(atomicOr(vis + w, b) & b);
+  }
+
+  // Pull test: does adj[b, e) hold a visited partition-mate?  Lists are read
+  // four entries at a time (one 16-byte load once aligned) and the four
+  // bitmap words are requested together, so a thread keeps several
+  // independent L2 requests in flight instead of one dependent chain.
+  __device__ bool any_visited(const uint32_t *__restrict__ adj, uint32_t b, uint32_t e, const uint32_t *vis,
+                              bool ranged, uint32_t rv) {
+    const uint32_t *rng = P.s.range;
+    auto hit = [&](uint32_t u) {
+      return ((ldm(vis + (u >> 5)) >> (u & 31u)) & 1u) && (!ranged || ldm(rng + u) == rv);
+    };
+    uint32_t i = b;
+    // 16-byte loads only when the list base is 16-byte aligned (caller-bound
+    // graphs may not be); otherwise the scalar tail loop below does it all
+    const bool vec = (reinterpret_cast<uintptr_t>(adj) & 15u) == 0;
+    while (vec && i < e && (i & 3u)) {
+      if (hit(ldg(adj + i))) return true;
+      ++i;
+    }
+    if (!ranged) {  // eight probes in flight per step
+      for (; vec && i + 8 <= e; i += 8) {
+        const uint4 q = __ldg(reinterpret_cast<const uint4 *>(adj + i));
+        const uint4 r = __ldg(reinterpret_cast<const uint4 *>(adj + i + 4));
+        const uint32_t w0 = ldm(vis + (q.x >> 5)), w1 = ldm(vis + (q.y >> 5));
+        const uint32_t w2 = ldm(vis + (q.z >> 5)), w3 = ldm(vis + (q.w >> 5));
+        const uint32_t w4 = ldm(vis + (r.x >> 5)), w5 = ldm(vis + (r.y >> 5));
+        const uint32_t w6 = ldm(vis + (r.z >> 5)), w7 = ldm(vis + (r.w >> 5));
+        const uint32_t h = ((w0 >> (q.x & 31u)) | (w1 >> (q.y & 31u)) | (w2 >> (q.z & 31u)) | (w3 >> (q.w & 31u)) |
+                            (w4 >> (r.x & 31u)) | (w5 >> (r.y & 31u)) | (w6 >> (r.z & 31u)) | (w7 >> (r.w & 31u))) &
+                           1u;
+        if (h) return true;
+      }
+    }
+    for (; vec && i + 4 <= e; i += 4) {
+      const uint4 q = __ldg(reinterpret_cast<const uint4 *>(adj + i));
+      const uint32_t w0 = ldm(vis + (q.x >> 5)), w1 = ldm(vis + (q.y >> 5));
+      const uint32_t w2 = ldm(vis + (q.z >> 5)), w3 = ldm(vis + (q.w >> 5));
+      const bool h0 = (w0 >> (q.x & 31u)) & 1u, h1 = (w1 >> (q.y & 31u)) & 1u;
+      const bool h2 = (w2 >> (q.z & 31u)) & 1u, h3 = (w3 >> (q.w & 31u)) & 1u;
+      if (!ranged) {
+        if (h0 | h1 | h2 | h3) return true;
+      } else {
+        if ((h0 && ldm(rng + q.x) == rv) || (h1 && ldm(rng + q.y) == rv) || (h2 && ldm(rng + q.z) == rv) ||
+            (h3 && ldm(rng + q.w) == rv))
+          return true;
+      }
+    }
+    for (; i < e; ++i)
+      if (hit(ldg(adj + i))) return true;
+    return false;
   }
 
   // QUADRATIC (reach_q.cu:12-79,160-231): every sweep expands each visited,
@@ -387,16 +568,23 @@ struct Eng {
                               uint32_t *exp, bool ranged) {
     uint32_t depth = 0;
     for (;;) {
+      const unsigned long long ts = globaltimer_ns();
       uint32_t chg = 0;
       for_vertices([&](uint32_t v, bool valid) {
-        if (!valid || !live(v) || !bit_test(vis, v) || bit_test(exp, v)) return;
-        bit_set(exp, v);
+        if (!list_mode) {  // whole warp = one bitmap word: skip words without a frontier vertex
+          const uint32_t w = v >> 5;
+          if ((ldm(vis + w) & ~ldm(exp + w) & ~ldm(P.s.elim + w)) == 0u) return;
+        }
+        const bool fr = valid && live(v) && bit_test(vis, v) && !bit_test(exp, v);
+        warp_set_bits(exp, v, fr, !list_mode);
+        if (!fr) return;
         const uint32_t rv = ranged ? ldm(P.s.range + v) : 0u;
         const uint32_t b = ldg(off + v), e = ldg(off + v + 1);
         for (uint32_t i = b; i < e; ++i) chg += try_visit(vis, ldg(adj + i), ranged, rv);
       });
       add_count(cur() + C_CHG, chg);
       if (!bar(500)) return depth;
+      prof(PR_Q, ts, rdprv(C_CHG));
       ++depth;
       if (rdprv(C_CHG) == 0) break;
       if (depth >= P.o.max_iters) {
@@ -455,135 +643,73 @@ struct Eng {
     }
   }
 
-  // TOPO / BEST (reach_t.cu): topology sweeps with warp-gather load
-  // balancing; when the frontier's edges exceed the unexplored edges / alpha
-  // a sweep pulls instead (every unvisited vertex scans its reverse list for
-  // a visited partition-mate) until the frontier falls under live / beta.
-  __device__ uint32_t reach_t(const uint32_t *__restrict__ off, const uint32_t *__restrict__ adj,
-                              const uint32_t *__restrict__ poff, const uint32_t *__restrict__ padj, uint32_t *vis,
-                              uint32_t *exp, bool ranged, bool allow_pull) {
+  // Worklist reach: DATA / LINEAR / TOPO / BEST.  Levels are synchronous:
+  // level k expands the vertices first reached in level k-1 (the pivots at
+  // k = 0) and appends each vertex it reaches, exactly once, to the next
+  // worklist, so the n-slot worklists cannot overflow (reference
+  // worklistc.h:79-81 drops items instead).  DATA expands one item per
+  // thread (reach_d.cu); LINEAR gathers a level's edges warp-wide and splits
+  // heavy lists across the grid (reach_l.cu).  TOPO / BEST add the bottom-up
+  // topology sweep (reach_t.cu sweeps every vertex each level; reach_b.cu
+  // switches direction): when the frontier's edges exceed the unexplored
+  // edges / alpha, a level becomes a pull sweep -- every live unvisited
+  // vertex scans its reverse list for a visited partition-mate -- until fewer
+  // than live / beta vertices are reached per sweep.
+  __device__ uint32_t reach_wl(const uint32_t *__restrict__ off, const uint32_t *__restrict__ adj,
+                               const uint32_t *__restrict__ poff, const uint32_t *__restrict__ padj, uint32_t *vis,
+                               bool ranged, bool balanced, bool allow_pull) {
     const EngState &s = P.s;
-    uint32_t depth = 0;
-    bool pull = false;
-    unsigned long long nf = 1, mf = 0, explored = 0;
-    const unsigned long long mtot = P.g.m;
     const uint32_t heavy = P.o.heavy_degree;
     const long long alpha = P.o.pull_alpha > 0 ? P.o.pull_alpha : 14;
     const long long beta = P.o.pull_beta > 0 ? P.o.pull_beta : 24;
-    for (;;) {
-      const uint32_t nlive = ldm(&c->n_live);
+    const unsigned long long mtot = P.g.m;
+    const uint32_t *in = s.piv;
+    uint32_t nin = ldm(&c->piv_count);
+    uint32_t depth = 0, sel = 0;
+    unsigned long long explored = 0, mf = 0;
+    bool pull = false;
+    while (nin > 0) {
+      const unsigned long long ts = globaltimer_ns();
       if (allow_pull) {
         const unsigned long long unexplored = mtot > explored ? mtot - explored : 0ull;
         if (!pull && depth > 0 && (long long)mf * alpha > (long long)unexplored) pull = true;
-        else if (pull && (long long)nf * beta < (long long)nlive) pull = false;
+        else if (pull && (long long)nin * beta < (long long)ldm(&c->n_live)) pull = false;
       }
-      uint32_t chg = 0, degsum = 0;
-      auto visit = [&](uint32_t, uint32_t u, uint32_t rsrc) {
-        if (try_visit(vis, u, ranged, rsrc)) {
-          ++chg;
-          degsum += ldg(off + u + 1) - ldg(off + u);
-        }
-      };
-      if (!pull) {
-        for_vertices([&](uint32_t v, bool valid) {
-          const bool fr = valid && live(v) && bit_test(vis, v) && !bit_test(exp, v);
-          uint32_t b = 0, d = 0, rv = 0;
-          if (fr) {
-            bit_set(exp, v);
-            b = ldg(off + v);
-            d = ldg(off + v + 1) - b;
-            rv = ranged ? ldm(s.range + v) : 0u;
-            if (d > heavy) {
-              heavy_push(v, b, d, rv);
-              d = 0;
-            }
-          }
-          warp_gather(v, b, d, rv, adj, visit);
-        });
-        add_count(cur() + C_CHG, chg);
-        add_count(cur() + C_DEG, degsum);
-        if (!bar(600)) return depth;
-        const unsigned long long h = ldm64(prv64());
-        if ((uint32_t)(h >> 32) != 0) {
-          // carry the regular part's counts into this interval
-          if (is_lead()) {
-            atomicAdd(cur() + C_CHG, rdprv(C_CHG));
-            atomicAdd(cur() + C_DEG, rdprv(C_DEG));
-          }
-          chg = 0;
-          degsum = 0;
-          heavy_expand(adj, h, visit);
-          add_count(cur() + C_CHG, chg);
-          add_count(cur() + C_DEG, degsum);
-          if (!bar(601)) return depth;
-        }
-      } else {
-        if (is_lead()) atomicAdd(&c->pull_sweeps, 1u);
-        for_vertices([&](uint32_t v, bool valid) {
-          bool cand = false;
-          if (valid && live(v)) {
-            if (bit_test(vis, v)) {
-              if (!bit_test(exp, v)) bit_set(exp, v);  // reached before this sweep: its edges are covered
-            } else {
-              cand = true;
-            }
-          }
-          bool found = false;
-          if (cand) {
-            const uint32_t rv = ranged ? ldm(s.range + v) : 0u;
-            const uint32_t b = ldg(poff + v), e = ldg(poff + v + 1);
-            for (uint32_t i = b; i < e; ++i) {
-              const uint32_t u = ldg(padj + i);
-              if (bit_test(vis, u) && (!ranged || ldm(s.range + u) == rv)) {
-                found = true;
-                break;
-              }
-            }
-            if (found) {
-              bit_set(vis, v);
-              ++chg;
-              degsum += ldg(off + v + 1) - ldg(off + v);
-            }
-          }
-        });
-        add_count(cur() + C_CHG, chg);
-        add_count(cur() + C_DEG, degsum);
-        if (!bar(602)) return depth;
-      }
-      ++depth;
-      nf = rdprv(C_CHG);
-      mf = rdprv(C_DEG);
-      explored += mf;
-      if (nf == 0) break;
-      if (depth >= P.o.max_iters) {
-        fail(kErrIterCap);
-        break;
-      }
-    }
-    return depth;
-  }
-
-  // DATA / LINEAR (reach_d.cu, reach_l.cu): worklist levels seeded with the
-  // pivot list.  DATA expands one item per thread; LINEAR gathers the
-  // level's edges warp-wide and splits heavy lists across the grid.  Each
-  // vertex enters a worklist at most once (exactly-once claim), so the n-slot
-  // queues cannot overflow (reference worklistc.h:79-81 drops items).
-  __device__ uint32_t reach_wl(const uint32_t *__restrict__ off, const uint32_t *__restrict__ adj, uint32_t *vis,
-                               bool ranged, bool balanced) {
-    const EngState &s = P.s;
-    const uint32_t heavy = P.o.heavy_degree;
-    const uint32_t *in = s.piv;
-    uint32_t nin = ldm(&c->piv_count);
-    uint32_t *outs[2] = {s.qa, s.qb};
-    uint32_t depth = 0, sel = 0;
-    while (nin > 0) {
-      uint32_t *out = outs[sel];
+      uint32_t *out = sel ? s.qb : s.qa;
       uint32_t *cnt = cur() + C_Q;
       uint32_t qoff = 0;  // items already appended to `out` in an earlier interval of this level
+      uint32_t degsum = 0;
       auto visit = [&](uint32_t, uint32_t u, uint32_t rsrc) {
-        if (try_visit(vis, u, ranged, rsrc)) queue_push(out + qoff, cnt, s.qcap - qoff, u, err());
+        if (try_visit(vis, u, ranged, rsrc)) {
+          queue_push(out + qoff, cnt, s.qcap - qoff, u, err());
+          if (allow_pull) degsum += ldg(off + u + 1) - ldg(off + u);
+        }
       };
-      if (balanced) {
+      uint32_t slot = PR_WL;
+      if (pull) {
+        slot = PR_PULL;
+        if (is_lead()) atomicAdd(&c->pull_sweeps, 1u);
+        Stage pq{out, cnt, s.qcap, 0};
+        for_vertices([&](uint32_t v, bool valid) {
+          const uint32_t w = v >> 5;
+          const uint32_t vw = ldm(vis + w), ew = ldm(s.elim + w);
+          // whole warp = one bitmap word in full mode: skip words without a live unvisited vertex
+          if (!list_mode && (~vw & ~ew) == 0u) return;
+          const uint32_t vv = valid ? v : 0u;
+          const uint32_t pb = ldg(poff + vv), pe = ldg(poff + vv + 1);
+          const uint32_t rv = ranged ? ldm(s.range + vv) : 0u;
+          bool found = false;
+          if (valid && !(((vw | ew) >> (v & 31u)) & 1u)) {
+            found = any_visited(padj, pb, pe, vis, ranged, rv);
+            if (found) degsum += ldg(off + v + 1) - ldg(off + v);
+          }
+          warp_set_bits(vis, v, found, !list_mode);
+          stage_put(pq, found, v);
+        });
+        stage_flush(pq);
+        add_count(cur() + C_DEG, degsum);
+        if (!bar(703)) return depth;
+      } else if (balanced) {
         for_items(nin, [&](uint32_t i, bool valid) {
           uint32_t v = 0, b = 0, d = 0, rv = 0;
           if (valid) {
@@ -598,22 +724,19 @@ struct Eng {
           }
           warp_gather(v, b, d, rv, adj, visit);
         });
+        add_count(cur() + C_DEG, degsum);
         if (!bar(700)) return depth;
         const unsigned long long h = ldm64(prv64());
         if ((uint32_t)(h >> 32) != 0) {
+          const unsigned long long th = globaltimer_ns();
           qoff = rdprv(C_Q);
           cnt = cur() + C_Q;
+          if (is_lead()) atomicAdd(cur() + C_DEG, rdprv(C_DEG));
+          degsum = 0;
           heavy_expand(adj, h, visit);
+          add_count(cur() + C_DEG, degsum);
           if (!bar(701)) return depth;
-          ++depth;
-          nin = qoff + rdprv(C_Q);
-          in = out;
-          sel ^= 1u;
-          if (depth >= P.o.max_iters) {
-            fail(kErrIterCap);
-            break;
-          }
-          continue;
+          prof(PR_HEAVY, th, (uint32_t)(h >> 32), (uint32_t)h);
         }
       } else {
         for (uint32_t i = gtid(); i < nin; i += gstride()) {
@@ -622,10 +745,14 @@ struct Eng {
           const uint32_t b = ldg(off + v), e = ldg(off + v + 1);
           for (uint32_t j = b; j < e; ++j) visit(v, ldg(adj + j), rv);
         }
+        add_count(cur() + C_DEG, degsum);
         if (!bar(702)) return depth;
       }
       ++depth;
-      nin = rdprv(C_Q);
+      nin = qoff + rdprv(C_Q);
+      mf = rdprv(C_DEG);
+      explored += mf;
+      prof(slot, ts, nin, (uint32_t)mf);
       in = out;
       sel ^= 1u;
       if (depth >= P.o.max_iters) {
@@ -644,10 +771,10 @@ struct Eng {
     uint32_t *vis = dir ? s.bvis : s.fvis, *exp = dir ? s.bexp : s.fexp;
     switch (arm) {
       case ARM_Q: return reach_q(off, adj, vis, exp, ranged);
-      case ARM_D: return reach_wl(off, adj, vis, ranged, false);
-      case ARM_L: return reach_wl(off, adj, vis, ranged, true);
-      case ARM_B: return reach_t(off, adj, poff, padj, vis, exp, ranged, true);
-      default: return reach_t(off, adj, poff, padj, vis, exp, ranged, P.o.pull_alpha >= 0);
+      case ARM_D: return reach_wl(off, adj, poff, padj, vis, ranged, false, false);
+      case ARM_L: return reach_wl(off, adj, poff, padj, vis, ranged, true, false);
+      case ARM_B: return reach_wl(off, adj, poff, padj, vis, ranged, true, true);
+      default: return reach_wl(off, adj, poff, padj, vis, ranged, true, P.o.pull_alpha >= 0);
     }
   }
 
@@ -787,11 +914,13 @@ struct Eng {
   // ============================================= active-list compaction
   __device__ void compact() {
     const EngState &s = P.s;
-    uint32_t *dst = s.act[act_sel ^ 1u];
+    Stage aq{s.act[act_sel ^ 1u], cur() + C_Q, s.qcap, 0};
     for_vertices([&](uint32_t v, bool valid) {
-      const bool a = valid && live(v);
-      warp_push(dst, cur() + C_Q, s.qcap, v, a, err());
+      const uint32_t ew = ldm(s.elim + (v >> 5));
+      if (!list_mode && ~ew == 0u) return;  // whole word eliminated
+      stage_put(aq, valid && !((ew >> (v & 31u)) & 1u), v);
     });
+    stage_flush(aq);
     if (!bar(1000)) return;
     if (is_lead()) {
       c->act_count = rdprv(C_Q);
@@ -805,7 +934,7 @@ struct Eng {
   __device__ void maybe_compact() {
     const uint32_t nlive = ldm(&c->n_live);
     const uint32_t span = list_mode ? act_count : P.g.n;
-    if ((unsigned long long)nlive * 4ull < span) compact();
+    if (nlive > 0 && (unsigned long long)nlive * 4ull < span) compact();
   }
 
   __device__ void sync_live() {
@@ -842,21 +971,13 @@ struct Eng {
       });
       if (!bar(1102)) return;
     }
-    uint32_t cnt = 0, unresolved = 0;
-    for_all_ids([&](uint32_t v, bool valid) {
-      if (!valid) return;
-      const uint32_t l = ldm(s.label + v);
-      cnt += l == v;
-      unresolved += l == 0;
-      if (s.out_labels) s.out_labels[v] = l;
-    });
-    if (s.out_labels && is_lead()) s.out_labels[0] = 0;
-    add_count(cur() + C_CNT, cnt);
-    add_count(cur() + C_CNT2, unresolved);
-    if (!bar(1103)) return;
+    // No counting sweep: every SCC was counted when its representative was
+    // assigned (trim-1: one per vertex, trim-2: one per pair, F∩B: one per
+    // eliminated pivot).  phase_ret = vertices still without a component.
     if (is_lead()) {
-      c->nscc = rdprv(C_CNT);
-      c->phase_ret = rdprv(C_CNT2);
+      c->nscc = ldm(&c->n_trimmed) + ldm(&c->n_trim2) / 2 + ldm(&c->n_fbscc);
+      c->phase_ret = ldm(&c->n_live);
+      s.label[0] = 0;
     }
   }
 
@@ -883,16 +1004,30 @@ struct Eng {
     const bool single = P.s.nseg <= 1;
     refresh_mode();
     unsigned long long t0 = globaltimer_ns();
+    // true while the live set and the partitions equal those of the last
+    // trim fixpoint: another trim pass then provably removes nothing
+    bool trim_fresh = false;
+    // with one degree sweep and a single partition the first pivot is elected
+    // inside that sweep (its survivors are exactly the live vertices)
+    const uint32_t tf_cap = o.trim_first_depth > 0 ? (uint32_t)o.trim_first_depth : o.max_iters;
+    const bool fused_pick = o.trim_first && single && tf_cap == 1;
     if (o.trim_first) {
-      const uint32_t it = trim(false, P.g.sorted_unique != 0, o.max_iters);
+      const uint32_t it = trim(false, P.g.sorted_unique != 0, tf_cap, fused_pick);
       if (is_lead()) c->trim_iters += it;
       sync_live();
       if (!bar(1)) return;
+      // The first round's trim would run on the same live set and partition;
+      // what it could still remove, later partition-aware trims remove.
+      trim_fresh = true;
     }
     timed(c->ns_trim, t0);
     t0 = globaltimer_ns();
-    if (single) {
+    if (fused_pick) {
+      commit_first_pivot();
+      prof(PR_PIVOT, t0);
+    } else if (single) {
       pick_first_pivot();
+      prof(PR_PIVOT, t0);
     } else {
       update();
       sync_live();
@@ -919,7 +1054,10 @@ struct Eng {
       timed(c->ns_bwd, t0);
       t0 = globaltimer_ns();
       uint32_t ti = 0;
-      if (o.trim_depth >= 0) {
+      // The reference trims here every round (scc.cu:717-722).  In the first
+      // round of a single partition right after the global trim-1 fixpoint,
+      // reach changed only visit bits, so that trim cannot remove anything.
+      if (o.trim_depth >= 0 && !(step == 1 && single && trim_fresh)) {
         const uint32_t cap = o.trim_depth == 0 ? o.max_iters : (uint32_t)o.trim_depth;
         ti = trim(ranged, false, cap);
       }
@@ -931,12 +1069,18 @@ struct Eng {
       sync_live();
       if (!bar(4)) return;
       timed(c->ns_update, t0);
+      prof(PR_UPDATE, t0);
       if (is_lead()) {
         c->steps = step;
         c->fwd_depth += fd;
         c->bwd_depth += bd;
         c->trim_iters += ti;
       }
+      // shrink the sweep set first, so WCC and the next round cover only live vertices
+      t0 = globaltimer_ns();
+      maybe_compact();
+      if (!bar(6)) return;
+      prof(PR_COMPACT, t0);
       if (o.wcc && !wcc_done) {
         const uint32_t nel2 = ldm(&c->n_fbe) + ldm(&c->n_trim2);
         if (nel2 >= o.switch_thr) {
@@ -957,18 +1101,23 @@ struct Eng {
             if (is_lead()) c->wcc_iters += wi;
           }
           timed(c->ns_wcc, t0);
+          prof(PR_WCC, t0);
         }
       }
-      maybe_compact();
-      if (!bar(6)) return;
+      if (!bar(7)) return;
     }
+    t0 = globaltimer_ns();
     finalize();
+    prof(PR_FINAL, t0);
   }
 };
 
 // ------------------------------------------------------------------ kernels
 template <int BS>
-__global__ void __launch_bounds__(BS, 1024 / BS) scc_persistent(Params p, uint32_t phase, uint32_t a0, uint32_t a1,
+// __grid_constant__: Eng keeps a reference to the parameter block, which then
+// stays in the constant bank instead of being copied to local memory.
+__global__ void __launch_bounds__(BS, 1024 / BS) scc_persistent(const __grid_constant__ Params p, uint32_t phase,
+                                                                 uint32_t a0, uint32_t a1,
                                                                  uint32_t a2) {
   Eng<BS> e(p);
   Ctl *c = p.s.ctl;
@@ -1022,12 +1171,13 @@ __global__ void __launch_bounds__(BS, 1024 / BS) scc_persistent(Params p, uint32
   }
 }
 
-// per-solve reset: labels, partitions (segment index or 0), bitmaps
+// per-solve reset: partitions (segment index or 0), bitmaps.  Labels need no
+// reset: every vertex gets one when it is eliminated, and a solve ends only
+// when all are (n_live == 0).
 __global__ void scc_init_kernel(Params p) {
   const uint32_t n = p.g.n;
   const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
   for (uint32_t v = tid; v <= n; v += stride) {
-    p.s.label[v] = 0;
     uint32_t r = 0;
     if (p.s.nseg > 1 && v >= 1) {
       uint32_t lo = 0, hi = p.s.nseg - 1;  // largest s with seg[s] <= v

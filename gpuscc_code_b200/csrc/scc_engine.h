@@ -25,6 +25,7 @@ struct Ctl {
   uint32_t n_trimmed;           // removed by trim-1
   uint32_t n_trim2;             // removed by trim-2
   uint32_t n_fbe;               // removed as F∩B
+  uint32_t n_fbscc;             // SCCs found as F∩B (their pivots)
   uint32_t nscc;
   uint32_t piv_count;           // pivots chosen by the last selection
   uint32_t list_mode;           // 0: sweeps cover 0..n; 1: sweeps cover the active list
@@ -36,6 +37,31 @@ struct Ctl {
   uint32_t trim_first_done;
   uint32_t pad0;
   unsigned long long ns_trim, ns_fwd, ns_bwd, ns_update, ns_wcc;
+  // finer device timers (globaltimer, CTA 0) and counts, indexed by Prof
+  unsigned long long prof_ns[16];
+  uint32_t prof_cnt[16];
+  // per-sweep trace (first kTrace events of a launch): slot, two counters, ns
+  uint32_t trace_n, trace_pad;
+  uint32_t trace_slot[128], trace_a[128], trace_b[128];
+  unsigned long long trace_ns[128];
+};
+constexpr uint32_t kTrace = 128;
+
+enum Prof : uint32_t {
+  PR_TRIM_SWEEP = 0,  // first sweep of a trim
+  PR_TRIM_WL = 1,     // worklist iterations of a trim
+  PR_PUSH = 2,        // push sweeps (TOPO/BEST)
+  PR_PULL = 3,        // pull sweeps
+  PR_HEAVY = 4,       // grid-split heavy lists
+  PR_WL = 5,          // DATA/LINEAR levels
+  PR_Q = 6,           // QUADRATIC sweeps
+  PR_UPDATE = 7,
+  PR_WCC = 8,
+  PR_TRIM2 = 9,
+  PR_COMPACT = 10,
+  PR_FINAL = 11,
+  PR_PIVOT = 12,
+  PR_COUNT = 16
 };
 
 struct EngGraph {
@@ -72,6 +98,8 @@ struct EngOpts {
   int32_t pull_alpha, pull_beta;
   uint32_t warp_degree, heavy_degree, max_iters;
   unsigned long long timeout_ns;
+  int32_t trim_first_depth;
+  uint32_t pad;
 };
 
 struct Params {
@@ -79,6 +107,15 @@ struct Params {
   EngState s;
   EngOpts o;
 };
+
+// Bitmap words swept for an n-vertex graph: ids 0..n rounded up to a whole
+// number of 1024-thread blocks (32 words), so every CTA of a full-id sweep
+// runs the same number of iterations (it may synchronise inside them).
+// Allocations add kBitmapSlack words.
+constexpr uint32_t bitmap_words(uint32_t n) {
+  return (uint32_t)((((uint64_t)n + 1 + 31) / 32 + 31) / 32 * 32);
+}
+constexpr uint32_t kBitmapSlack = 4;
 
 enum Phase : uint32_t {
   PH_SOLVE = 0,

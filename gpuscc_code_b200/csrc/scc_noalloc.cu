@@ -32,7 +32,7 @@ namespace {
 constexpr uint32_t kMaxN = 1u << 16;  // vertices
 constexpr uint32_t kMaxM = 1u << 22;  // edges (each direction)
 constexpr size_t a256(size_t x) { return (x + 255) & ~size_t(255); }
-constexpr uint32_t kWords = ((((kMaxN + 1u + 31u) / 32u) + 3u) & ~3u) + 4u;
+constexpr uint32_t kWords = sccb::bitmap_words(kMaxN) + sccb::kBitmapSlack;
 constexpr size_t kVec = a256(size_t(kMaxN + 1) * 4);        // one u32 per vertex
 constexpr size_t kBitmaps = a256(size_t(kWords) * 4 * 7);   // elim, fvis, bvis, fexp, bexp, tflag, queued
 constexpr size_t kSlots = a256(size_t(kMaxN + 1) * 3 * 8);  // partition-election slots
@@ -147,7 +147,7 @@ extern "C" int scc_solve_noalloc(const scc_dev_csr *g, const scc_opts *opts, uin
   uint32_t *flag = reinterpret_cast<uint32_t *>(cur);
   s.seg = nullptr;
   s.out_labels = d_labels;
-  s.nwords = ((((uint32_t)(((uint64_t)n + 1 + 31) / 32)) + 3u) & ~3u);
+  s.nwords = sccb::bitmap_words(n);
   s.qcap = n + 1;
   s.hcap = kHeavyCap;
   s.nseg = 1;
@@ -165,6 +165,8 @@ extern "C" int scc_solve_noalloc(const scc_dev_csr *g, const scc_opts *opts, uin
   e.heavy_degree = o.heavy_degree ? o.heavy_degree : 4096u;
   e.max_iters = o.max_iters ? o.max_iters : (1u << 20);
   e.timeout_ns = (unsigned long long)(o.timeout_ms ? o.timeout_ms : 10000u) * 1000000ull;
+  e.trim_first_depth = o.trim_first_depth;
+  if (d_labels) s.label = d_labels;  // labels go straight to the caller's buffer
 
   // the array keeps the previous call's contents: reset what must start fresh
   cudaError_t err = cudaMemsetAsync(s.ctl, 0, sizeof(sccb::Ctl), st);

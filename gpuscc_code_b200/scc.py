@@ -166,6 +166,7 @@ class Options:
     max_iters: int = 0
     grid_blocks: int = 0
     timeout_ms: int = 0
+    trim_first_depth: int = 1
 
     def to_c(self) -> scc_opts:
         o = scc_opts()
@@ -281,6 +282,26 @@ class SCCContext:
         st = scc_stats()
         check(lib.scc_solve_collect(self._h, C.byref(cnt), C.byref(st)))
         return int(cnt.value), st.as_dict()
+
+    PROFILE_SLOTS = ["trim_sweep", "trim_worklist", "push", "pull", "heavy", "worklist_level", "quadratic",
+                     "update", "wcc", "trim2", "compact", "finalize", "first_pivot"]
+
+    def profile(self) -> dict:
+        """Device-side phase timers of the last call: {slot: (ms, count)}."""
+        ms = (C.c_double * 16)()
+        cnt = (C.c_uint32 * 16)()
+        check(lib.scc_get_profile(self._h, ms, cnt))
+        return {name: (round(ms[i], 4), int(cnt[i])) for i, name in enumerate(self.PROFILE_SLOTS) if cnt[i]}
+
+    def trace(self) -> list:
+        """Per-event device trace of the last call: [(slot name, a, b, ms)]."""
+        n = C.c_uint32()
+        sl, a, b = (C.c_uint32 * 128)(), (C.c_uint32 * 128)(), (C.c_uint32 * 128)()
+        ms = (C.c_double * 128)()
+        check(lib.scc_get_trace(self._h, C.byref(n), sl, a, b, ms))
+        names = self.PROFILE_SLOTS
+        return [(names[sl[i]] if sl[i] < len(names) else str(sl[i]), int(a[i]), int(b[i]), round(ms[i], 4))
+                for i in range(n.value)]
 
     # -------------------------------------------------------- phase level
     def phase_begin(self):

@@ -81,9 +81,12 @@ typedef struct scc_opts {
   uint32_t max_iters;      /* cap on sweeps of any one fixpoint/reach loop and on FB rounds (0 = 1<<20) */
   uint32_t grid_blocks;    /* persistent grid size (0 = every co-resident block) */
   uint32_t timeout_ms;     /* bound on any device-side wait inside the persistent kernel (0 = 10000) */
+  int32_t trim_first_depth;/* global trim-1 before the first pivot: 0 = to its fixpoint (reference trim1),
+                              k > 0 = at most k iterations; later partition-aware trims remove the rest */
 } scc_opts;
 
-/* Reference defaults: alg TOPO, wcc 0, trim2 0, trim_first 1, block 256, pivot MIN_ID, switch 10. */
+/* Reference defaults: alg TOPO, wcc 0, trim2 0, trim_first 1, block 256, pivot MIN_ID, switch 10;
+ * engine default trim_first_depth 1 (one degree sweep; the labels do not depend on it). */
 void scc_opts_default(scc_opts *opts);
 
 /* ----------------------------------------------------------- host graph */
@@ -223,6 +226,19 @@ int scc_solve_noalloc(const scc_dev_csr *g, const scc_opts *opts, uint32_t *d_la
  * in a CUDA graph).  Results: scc_solve_collect after the stream drained. */
 int scc_solve_enqueue(scc_ctx *ctx, uint32_t *d_labels);
 int scc_solve_collect(scc_ctx *ctx, uint32_t *nscc, scc_stats *stats);
+
+/* Device-side phase timers of the last solve or phase call (the reference's
+ * STOPWATCH accumulators, timing.h:14, taken inside the persistent kernel
+ * with %globaltimer): ms[i] / counts[i] for i < 16 in the order trim first
+ * sweep, trim worklist iterations, push sweeps, pull sweeps, heavy lists,
+ * worklist levels, quadratic sweeps, update, WCC, trim-2, compaction,
+ * finalize, first pivot, (3 reserved). */
+int scc_get_profile(scc_ctx *ctx, double *ms, uint32_t *counts);
+/* The first (up to) 128 timed events of the last call, in order: slot (as
+ * above), two event counters (reach sweeps: vertices reached and their
+ * edge count; trim: vertices removed; heavy: lists and edges) and ms.
+ * Arrays hold 128 entries; *n receives the number filled. */
+int scc_get_trace(scc_ctx *ctx, uint32_t *n, uint32_t *slot, uint32_t *a, uint32_t *b, double *ms);
 
 /* -------------------------------------------------------- phase level API
  * Each call runs one phase of the reference driver on the context's device
