@@ -236,7 +236,11 @@ def run_ours(args) -> None:
     import gpuscc_code_b200 as scc
 
     scale, samples = args.scale, 1 << args.samples_log2
-    opts = scc.Options(alg="h", wcc=True, trim2=True)
+    overrides = {}
+    for kv in args.opt:
+        k, v = kv.split("=", 1)
+        overrides[k] = v if k == "alg" else int(v)
+    opts = scc.Options(**{"alg": "h", "wcc": True, "trim2": True, **overrides})
     ctx = scc.SCCContext(local, opts)
     d = ctx.gen_rmat_device(scale, samples, ABC, args.seed)
     n, m = int(d.n), int(d.m)
@@ -341,7 +345,8 @@ def run_ours(args) -> None:
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u32", "data": "synthetic (R-MAT generated on the device, seed 2)",
         "config": workload_config(scale, args.samples_log2, args.seed,
-                                  {"n": n, "m": m, "nscc": cnt, "parallelism": f"replicas{world}"}),
+                                  {"n": n, "m": m, "nscc": cnt, "parallelism": f"replicas{world}",
+                                   "engine_overrides": overrides}),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
                      "kernel": "scc_persistent<256> (+ per-step init pass)", "kernel_ms": kern_ms,
@@ -373,6 +378,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--trace", action="store_true", help="include the per-sweep device trace in the line")
+    ap.add_argument("--opt", action="append", default=[], metavar="KEY=VALUE",
+                    help="override an engine option (scc_opts field), e.g. --opt occupancy=3")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

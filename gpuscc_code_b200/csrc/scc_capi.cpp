@@ -110,6 +110,8 @@ int check_opts(const scc_opts *o) {
   if (o->switch_permille < 0 || o->switch_permille > 1000)
     return set_error(SCC_ERR_INVALID, "switch_permille must be in 0..1000");
   if (o->heavy_degree != 0 && o->heavy_degree < 256) return set_error(SCC_ERR_INVALID, "heavy_degree must be >= 256");
+  if (o->occupancy != 0 && o->occupancy != 3 && o->occupancy != 4)
+    return set_error(SCC_ERR_INVALID, "occupancy must be 0, 3 or 4");
   return SCC_OK;
 }
 
@@ -243,7 +245,8 @@ int read_ctl(scc_ctx *c) {
 int launch(scc_ctx *c, uint32_t phase, uint32_t a0 = 0, uint32_t a1 = 0, uint32_t a2 = 0,
            uint32_t *out_labels = nullptr) {
   const sccb::Params p = make_params(c, out_labels);
-  CK(sccb::launch_phase(p, phase, a0, a1, a2, block_size_of(c), c->opts.grid_blocks, c->stream, &c->grid_used),
+  CK(sccb::launch_phase(p, phase, a0, a1, a2, block_size_of(c), c->opts.grid_blocks, c->stream, &c->grid_used,
+                        c->opts.occupancy),
      "cooperative launch");
   ++c->launches;
   return SCC_OK;

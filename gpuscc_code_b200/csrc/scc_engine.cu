@@ -140,6 +140,35 @@ struct Eng {
     for_vertices(f, [] {});
   }
 
+  // for_vertices with a one-deep software pipeline: load(v, valid) issues
+  // the loads of the NEXT iteration before f(v, valid, pre) runs on the
+  // current one, so their latency overlaps the current vertex's dependent
+  // chain.  load() may only read data that f() of the same iteration does
+  // not change for other lanes' vertices (bitmap words, offsets, ranges).
+  template <class L, class F>
+  __device__ void for_vertices_pf(L &&load, F &&f) {
+    if (list_mode) {
+      for_vertices([&](uint32_t v, bool valid) { f(v, valid, load(v, valid)); });
+      return;
+    }
+    const uint32_t lim = P.s.nwords * 32u;
+    const uint32_t n = P.g.n;
+    uint32_t base = blockIdx.x * BS;
+    if (base >= lim) return;
+    auto pre = load(base + threadIdx.x, base + threadIdx.x >= 1 && base + threadIdx.x <= n);
+    for (; base < lim; base += gstride()) {
+      const uint32_t v = base + threadIdx.x;
+      const uint32_t nb = base + gstride();
+      auto nxt = pre;
+      if (nb < lim) {
+        const uint32_t nv = nb + threadIdx.x;
+        nxt = load(nv, nv >= 1 && nv <= n);
+      }
+      f(v, v >= 1 && v <= n, pre);
+      pre = nxt;
+    }
+  }
+
   // Warp-staged worklist append.  Items a warp emits during a sweep collect
   // in its own shared-memory segment and reach the global list kStage at a
   // time with one atomicAdd, so a sweep that emits millions of items does not
@@ -235,14 +264,20 @@ struct Eng {
     uint32_t ntrim = 0;
     unsigned long long best = ~0ull;
     Stage tq{s.qa, cur() + C_Q, s.qcap, 0};
-    for_vertices([&](uint32_t v, bool valid) {
-      const uint32_t ew = ldm(s.elim + (v >> 5));
-      if (!list_mode && ~ew == 0u) return;  // whole word already eliminated
+    struct Pre {
+      uint32_t ew, a0, a1, b0, b1;
+    };
+    // a word's elimination bits change only through its own warp in this sweep
+    auto load = [&](uint32_t v, bool valid) {
       const uint32_t vv = valid ? v : 0u;
+      return Pre{ldm(s.elim + (v >> 5)), ldg(g.off + vv), ldg(g.off + vv + 1), ldg(g.offT + vv),
+                 ldg(g.offT + vv + 1)};
+    };
+    for_vertices_pf(load, [&](uint32_t v, bool valid, const Pre &p) {
+      const uint32_t ew = p.ew;
+      if (!list_mode && ~ew == 0u) return;  // whole word already eliminated
       const bool lv = valid && !((ew >> (v & 31u)) & 1u);
-      // all four offsets are requested before anything depends on them
-      const uint32_t a0 = ldg(g.off + vv), a1 = ldg(g.off + vv + 1);
-      const uint32_t b0 = ldg(g.offT + vv), b1 = ldg(g.offT + vv + 1);
+      const uint32_t a0 = p.a0, a1 = p.a1, b0 = p.b0, b1 = p.b1;
       bool t = false;
       if (lv) {
         if (snap) {  // nothing eliminated yet, lists sorted-unique: degrees decide
@@ -690,18 +725,23 @@ struct Eng {
         slot = PR_PULL;
         if (is_lead()) atomicAdd(&c->pull_sweeps, 1u);
         Stage pq{out, cnt, s.qcap, 0};
-        for_vertices([&](uint32_t v, bool valid) {
-          const uint32_t w = v >> 5;
-          const uint32_t vw = ldm(vis + w), ew = ldm(s.elim + w);
+        struct Pre {
+          uint32_t vw, ew, pb, pe, ob, oe, rv;
+        };
+        // Only v's own lane sets v's visit bit during a pull sweep, so the
+        // prefetched word is current for the bit this lane tests.
+        auto load = [&](uint32_t v, bool valid) {
+          const uint32_t w = v >> 5, vv = valid ? v : 0u;
+          return Pre{ldm(vis + w),  ldm(s.elim + w),   ldg(poff + vv), ldg(poff + vv + 1),
+                     ldg(off + vv), ldg(off + vv + 1), ranged ? ldm(s.range + vv) : 0u};
+        };
+        for_vertices_pf(load, [&](uint32_t v, bool valid, const Pre &p) {
           // whole warp = one bitmap word in full mode: skip words without a live unvisited vertex
-          if (!list_mode && (~vw & ~ew) == 0u) return;
-          const uint32_t vv = valid ? v : 0u;
-          const uint32_t pb = ldg(poff + vv), pe = ldg(poff + vv + 1);
-          const uint32_t rv = ranged ? ldm(s.range + vv) : 0u;
+          if (!list_mode && (~p.vw & ~p.ew) == 0u) return;
           bool found = false;
-          if (valid && !(((vw | ew) >> (v & 31u)) & 1u)) {
-            found = any_visited(padj, pb, pe, vis, ranged, rv);
-            if (found) degsum += ldg(off + v + 1) - ldg(off + v);
+          if (valid && !(((p.vw | p.ew) >> (v & 31u)) & 1u)) {
+            found = any_visited(padj, p.pb, p.pe, vis, ranged, p.rv);
+            if (found) degsum += p.oe - p.ob;
           }
           warp_set_bits(vis, v, found, !list_mode);
           stage_put(pq, found, v);
@@ -1113,12 +1153,13 @@ struct Eng {
 };
 
 // ------------------------------------------------------------------ kernels
-template <int BS>
+// MINB: resident CTAs per SM the register allocation is sized for (the
+// 1024/BS variant caps registers at 64, the 768/BS one at 80).
 // __grid_constant__: Eng keeps a reference to the parameter block, which then
 // stays in the constant bank instead of being copied to local memory.
-__global__ void __launch_bounds__(BS, 1024 / BS) scc_persistent(const __grid_constant__ Params p, uint32_t phase,
-                                                                 uint32_t a0, uint32_t a1,
-                                                                 uint32_t a2) {
+template <int BS, int MINB>
+__global__ void __launch_bounds__(BS, MINB) scc_persistent(const __grid_constant__ Params p, uint32_t phase,
+                                                            uint32_t a0, uint32_t a1, uint32_t a2) {
   Eng<BS> e(p);
   Ctl *c = p.s.ctl;
   e.refresh_mode();
@@ -1269,7 +1310,7 @@ __global__ void scc_ranges_kernel(Params p, uint32_t *out) {
   }
 }
 
-template <int BS>
+template <int BS, int MINB>
 static cudaError_t coop_launch(const Params &p, uint32_t phase, uint32_t a0, uint32_t a1, uint32_t a2,
                                uint32_t grid_blocks, cudaStream_t stream, uint32_t *grid_used) {
   int dev = 0, sms = 0, per_sm = 0;
@@ -1277,7 +1318,7 @@ static cudaError_t coop_launch(const Params &p, uint32_t phase, uint32_t a0, uin
   if (e != cudaSuccess) return e;
   e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   if (e != cudaSuccess) return e;
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, scc_persistent<BS>, BS, 0);
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, scc_persistent<BS, MINB>, BS, 0);
   if (e != cudaSuccess) return e;
   if (per_sm < 1) return cudaErrorInvalidConfiguration;
   uint32_t maxg = (uint32_t)(sms * per_sm);
@@ -1285,34 +1326,26 @@ static cudaError_t coop_launch(const Params &p, uint32_t phase, uint32_t a0, uin
   if (grid_used) *grid_used = g;
   Params pp = p;
   void *args[] = {&pp, &phase, &a0, &a1, &a2};
-  return cudaLaunchCooperativeKernel((const void *)scc_persistent<BS>, dim3(g), dim3(BS), args, 0, stream);
+  return cudaLaunchCooperativeKernel((const void *)scc_persistent<BS, MINB>, dim3(g), dim3(BS), args, 0, stream);
+}
+
+template <int BS>
+static cudaError_t coop_launch_occ(const Params &p, uint32_t phase, uint32_t a0, uint32_t a1, uint32_t a2,
+                                   uint32_t grid_blocks, cudaStream_t stream, uint32_t *grid_used, int occupancy) {
+  constexpr int kHi = 1024 / BS;
+  constexpr int kLo = 768 / BS > 0 ? 768 / BS : 1;
+  if (occupancy == 3) return coop_launch<BS, kLo>(p, phase, a0, a1, a2, grid_blocks, stream, grid_used);
+  return coop_launch<BS, kHi>(p, phase, a0, a1, a2, grid_blocks, stream, grid_used);
 }
 
 cudaError_t launch_phase(const Params &p, uint32_t phase, uint32_t a0, uint32_t a1, uint32_t a2, int block_size,
-                         uint32_t grid_blocks, cudaStream_t stream, uint32_t *grid_used) {
+                         uint32_t grid_blocks, cudaStream_t stream, uint32_t *grid_used, int occupancy) {
   switch (block_size) {
-    case 128: return coop_launch<128>(p, phase, a0, a1, a2, grid_blocks, stream, grid_used);
-    case 512: return coop_launch<512>(p, phase, a0, a1, a2, grid_blocks, stream, grid_used);
-    case 1024: return coop_launch<1024>(p, phase, a0, a1, a2, grid_blocks, stream, grid_used);
-    default: return coop_launch<256>(p, phase, a0, a1, a2, grid_blocks, stream, grid_used);
+    case 128: return coop_launch_occ<128>(p, phase, a0, a1, a2, grid_blocks, stream, grid_used, occupancy);
+    case 512: return coop_launch_occ<512>(p, phase, a0, a1, a2, grid_blocks, stream, grid_used, occupancy);
+    case 1024: return coop_launch_occ<1024>(p, phase, a0, a1, a2, grid_blocks, stream, grid_used, occupancy);
+    default: return coop_launch_occ<256>(p, phase, a0, a1, a2, grid_blocks, stream, grid_used, occupancy);
   }
-}
-
-cudaError_t persistent_grid(int block_size, uint32_t *grid_blocks) {
-  int dev = 0, sms = 0, per_sm = 0;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess) return e;
-  e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  if (e != cudaSuccess) return e;
-  switch (block_size) {
-    case 128: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, scc_persistent<128>, 128, 0); break;
-    case 512: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, scc_persistent<512>, 512, 0); break;
-    case 1024: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, scc_persistent<1024>, 1024, 0); break;
-    default: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, scc_persistent<256>, 256, 0); break;
-  }
-  if (e != cudaSuccess) return e;
-  *grid_blocks = (uint32_t)(sms * per_sm);
-  return cudaSuccess;
 }
 
 cudaError_t launch_init(const Params &p, cudaStream_t stream) {

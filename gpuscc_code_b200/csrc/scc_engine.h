@@ -132,12 +132,12 @@ enum Phase : uint32_t {
 };
 
 // Launch helpers (implemented in scc_engine.cu).
-// Cooperative launch of the persistent kernel for `phase`.
+// Cooperative launch of the persistent kernel for `phase`; occupancy selects
+// the register budget (4: four 256-thread CTAs per SM, 64 registers; 3:
+// three CTAs, 80 registers).
 cudaError_t launch_phase(const Params &p, uint32_t phase, uint32_t a0, uint32_t a1, uint32_t a2,
                          int block_size, uint32_t grid_blocks, cudaStream_t stream,
-                         uint32_t *grid_used);
-// Occupancy-derived co-resident grid for the persistent kernel.
-cudaError_t persistent_grid(int block_size, uint32_t *grid_blocks);
+                         uint32_t *grid_used, int occupancy);
 // Per-solve reset of the per-vertex state (plain launch).
 cudaError_t launch_init(const Params &p, cudaStream_t stream);
 // states export in the reference bit encoding.

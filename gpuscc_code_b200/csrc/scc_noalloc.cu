@@ -181,7 +181,8 @@ extern "C" int scc_solve_noalloc(const scc_dev_csr *g, const scc_opts *opts, uin
   err = sccb::launch_init(p, st);
   if (err == cudaSuccess) {
     uint32_t grid = 0;
-    err = sccb::launch_phase(p, sccb::PH_SOLVE, 0, 0, 0, o.block_size ? o.block_size : 256, o.grid_blocks, st, &grid);
+    err = sccb::launch_phase(p, sccb::PH_SOLVE, 0, 0, 0, o.block_size ? o.block_size : 256, o.grid_blocks, st, &grid,
+                             o.occupancy);
   }
   sccb::Ctl hc;
   if (err == cudaSuccess) err = cudaMemcpyAsync(&hc, s.ctl, sizeof(hc), cudaMemcpyDeviceToHost, st);

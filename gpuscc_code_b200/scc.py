@@ -167,6 +167,7 @@ class Options:
     grid_blocks: int = 0
     timeout_ms: int = 0
     trim_first_depth: int = 1
+    occupancy: int = 0
 
     def to_c(self) -> scc_opts:
         o = scc_opts()

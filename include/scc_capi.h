@@ -83,6 +83,8 @@ typedef struct scc_opts {
   uint32_t timeout_ms;     /* bound on any device-side wait inside the persistent kernel (0 = 10000) */
   int32_t trim_first_depth;/* global trim-1 before the first pivot: 0 = to its fixpoint (reference trim1),
                               k > 0 = at most k iterations; later partition-aware trims remove the rest */
+  int32_t occupancy;       /* register budget of the persistent kernel: 4 = four 256-thread CTAs per SM
+                              (64 registers), 3 = three (80 registers); 0 = engine default (4) */
 } scc_opts;
 
 /* Reference defaults: alg TOPO, wcc 0, trim2 0, trim_first 1, block 256, pivot MIN_ID, switch 10;
