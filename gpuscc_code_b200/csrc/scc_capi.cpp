@@ -110,8 +110,8 @@ int check_opts(const scc_opts *o) {
   if (o->switch_permille < 0 || o->switch_permille > 1000)
     return set_error(SCC_ERR_INVALID, "switch_permille must be in 0..1000");
   if (o->heavy_degree != 0 && o->heavy_degree < 256) return set_error(SCC_ERR_INVALID, "heavy_degree must be >= 256");
-  if (o->occupancy != 0 && o->occupancy != 3 && o->occupancy != 4)
-    return set_error(SCC_ERR_INVALID, "occupancy must be 0, 3 or 4");
+  if (o->occupancy != 0 && (o->occupancy < 3 || o->occupancy > 6))
+    return set_error(SCC_ERR_INVALID, "occupancy must be 0 or 3..6");
   return SCC_OK;
 }
 

@@ -1335,6 +1335,10 @@ static cudaError_t coop_launch_occ(const Params &p, uint32_t phase, uint32_t a0,
   constexpr int kHi = 1024 / BS;
   constexpr int kLo = 768 / BS > 0 ? 768 / BS : 1;
   if (occupancy == 3) return coop_launch<BS, kLo>(p, phase, a0, a1, a2, grid_blocks, stream, grid_used);
+  if constexpr (BS == 256) {  // tighter register budgets, 256-thread CTAs only
+    if (occupancy == 5) return coop_launch<BS, 5>(p, phase, a0, a1, a2, grid_blocks, stream, grid_used);
+    if (occupancy == 6) return coop_launch<BS, 6>(p, phase, a0, a1, a2, grid_blocks, stream, grid_used);
+  }
   return coop_launch<BS, kHi>(p, phase, a0, a1, a2, grid_blocks, stream, grid_used);
 }
 
