@@ -5,7 +5,7 @@ include/scc_capi.h (libgpuscc_b200.so, built in-tree); this package is the
 Python host binding.  Importing it fails if the library is not built.
 """
 from ._capi import ALG, SCCError, lib  # noqa: F401  (raises ImportError when the .so is missing)
-from .scc import (HostCSR, Options, SCCContext, computeSCC, csr_from_edges, gen_er, gen_grid,  # noqa: F401
+from .scc import (HostCSR, Options, SCCContext, computeSCC, csr_from_edges, gen_batch, gen_er, gen_grid,  # noqa: F401
                   gen_rmat, load, tarjan)
 
 __version__ = lib.scc_version().decode()

@@ -98,6 +98,13 @@ SIGNATURES = [
     ("scc_solve_device", C.c_int, [C.c_void_p, C.c_void_p, u32p, C.POINTER(scc_stats)]),
     ("scc_solve_noalloc", C.c_int, [C.POINTER(scc_dev_csr), C.POINTER(scc_opts), C.c_void_p, u32p, C.c_void_p]),
     ("scc_solve_enqueue", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("scc_solve_capture", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("scc_solve_replay", C.c_int, [C.c_void_p, u32p, C.POINTER(scc_stats)]),
+    ("scc_read_labels", C.c_int, [C.c_void_p, u32p]),
+    ("scc_gen_batch", C.c_int, [C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint64,
+                                C.POINTER(scc_host_csr), u32p]),
+    ("scc_gen_batch_device", C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
+                                       C.c_uint64, C.POINTER(scc_dev_csr), u32p]),
     ("scc_solve_collect", C.c_int, [C.c_void_p, u32p, C.POINTER(scc_stats)]),
     ("scc_get_profile", C.c_int, [C.c_void_p, C.POINTER(C.c_double), u32p]),
     ("scc_get_trace", C.c_int, [C.c_void_p, u32p, u32p, u32p, u32p, C.POINTER(C.c_double)]),

@@ -82,6 +82,7 @@ struct scc_ctx {
   uint32_t grid_used = 0;
   uint32_t launches = 0;
   uint32_t *enq_labels = nullptr;
+  cudaGraphExec_t solve_exec = nullptr;  // captured solve (scc_solve_capture)
 };
 
 namespace {
@@ -255,7 +256,9 @@ int launch(scc_ctx *c, uint32_t phase, uint32_t a0 = 0, uint32_t a1 = 0, uint32_
 int reset_state(scc_ctx *c) {
   int rc = ensure_state(c);
   if (rc) return rc;
+  CK(cudaGetLastError(), "pending CUDA error before the solve");
   CK(cudaMemsetAsync(c->ctl.p, 0, sizeof(sccb::Ctl), c->stream), "clear control block");
+  CK(cudaGetLastError(), "clear control block (deferred)");
   const sccb::Params p = make_params(c, nullptr);
   CK(sccb::launch_init(p, c->stream), "init launch");
   ++c->launches;
@@ -355,6 +358,7 @@ int scc_ctx_destroy(scc_ctx *c) {
   if (c->h_ctl) cudaFreeHost(c->h_ctl);
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
+  if (c->solve_exec) cudaGraphExecDestroy(c->solve_exec);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return SCC_OK;
@@ -468,6 +472,52 @@ int scc_gen_rmat_device(scc_ctx *c, uint32_t scale, uint64_t samples, uint32_t a
     out->edgesT = adjT;
   }
   return ensure_state(c);
+}
+
+int scc_gen_batch_device(scc_ctx *c, uint32_t count, uint32_t n_lo, uint32_t n_hi, uint32_t deg_lo_milli,
+                         uint32_t deg_hi_milli, uint64_t seed, scc_dev_csr *out, uint32_t *seg_first) {
+  sccb::clear_error();
+  if (!c || !seg_first) return set_error(SCC_ERR_INVALID, "null argument");
+  std::vector<sccg::BatchGraph> plan;
+  int rc = sccb::plan_batch(count, n_lo, n_hi, deg_lo_milli, deg_hi_milli, seed, &plan);
+  if (rc) return rc;
+  rc = use_device(c);
+  if (rc) return rc;
+  for (DBuf *b : {&c->g_off, &c->g_adj, &c->g_offT, &c->g_adjT}) b->release();
+  c->have_graph = false;
+  uint32_t *off = nullptr, *adj = nullptr, *offT = nullptr, *adjT = nullptr, n = 0, m = 0;
+  CK(sccb::gen_batch_device(plan.data(), count, c->stream, &off, &adj, &offT, &adjT, &n, &m), "device batch build");
+  c->g_off.p = off;
+  c->g_off.bytes = ((size_t)n + 2) * 4;
+  c->g_adj.p = adj;
+  c->g_adj.bytes = ((size_t)m + 1) * 4;
+  c->g_offT.p = offT;
+  c->g_offT.bytes = ((size_t)n + 2) * 4;
+  c->g_adjT.p = adjT;
+  c->g_adjT.bytes = ((size_t)m + 1) * 4;
+  c->d_off = off;
+  c->d_adj = adj;
+  c->d_offT = offT;
+  c->d_adjT = adjT;
+  c->n = n;
+  c->m = m;
+  c->sorted_unique = 1;
+  c->have_graph = true;
+  c->phase_ready = false;
+  seg_first[0] = 1;
+  for (uint32_t g = 0; g < count; ++g) seg_first[g + 1] = seg_first[g] + plan[g].n;
+  if (out) {
+    out->n = n;
+    out->m = m;
+    out->sorted_unique = 1;
+    out->nodes = off;
+    out->edges = adj;
+    out->nodesT = offT;
+    out->edgesT = adjT;
+  }
+  rc = ensure_state(c);
+  if (rc) return rc;
+  return scc_ctx_set_segments(c, count, seg_first);
 }
 
 int scc_ctx_bind_device(scc_ctx *c, const scc_dev_csr *g) {
@@ -586,10 +636,15 @@ int scc_solve_enqueue(scc_ctx *c, uint32_t *d_labels) {
   c->launches = 0;
   rc = reset_state(c);
   if (rc) return rc;
-  CK(cudaEventRecord(c->ev0, c->stream), "event");  // ms_total: the persistent kernel alone
+  // ms_total: the persistent kernel alone.  Not recorded while the sequence
+  // is being captured (a replay times the whole graph launch instead).
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  CK(cudaStreamIsCapturing(c->stream, &cs), "capture status");
+  const bool timed = cs == cudaStreamCaptureStatusNone;
+  if (timed) CK(cudaEventRecord(c->ev0, c->stream), "event");
   rc = launch(c, sccb::PH_SOLVE, 0, 0, 0, d_labels);
   if (rc) return rc;
-  CK(cudaEventRecord(c->ev1, c->stream), "event");
+  if (timed) CK(cudaEventRecord(c->ev1, c->stream), "event");
   c->enq_labels = d_labels;
   c->phase_ready = false;
   return SCC_OK;
@@ -600,11 +655,74 @@ int scc_solve_collect(scc_ctx *c, uint32_t *nscc, scc_stats *st) {
   int rc = read_ctl(c);
   if (rc) return rc;
   float ms = 0.f;
-  cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+  CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1), "solve timing events");
   if (c->h_ctl->phase_ret != 0)
     return set_error(SCC_ERR_STATE, "%u vertices left without a component", c->h_ctl->phase_ret);
   if (nscc) *nscc = c->h_ctl->nscc;
   fill_stats(c, st, ms);
+  return SCC_OK;
+}
+
+int scc_solve_capture(scc_ctx *c, uint32_t *d_labels) {
+  sccb::clear_error();
+  int rc = need_graph(c);
+  if (rc) return rc;
+  rc = use_device(c);
+  if (rc) return rc;
+  CK(cudaGetLastError(), "pending CUDA error at capture entry");
+  rc = ensure_state(c);  // allocations and the slot reset happen before capture
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(c->stream), "pre-capture sync");
+  if (c->solve_exec) {
+    cudaGraphExecDestroy(c->solve_exec);
+    c->solve_exec = nullptr;
+  }
+  CK(cudaGetLastError(), "pending CUDA error before capture");
+  CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+  CK(cudaGetLastError(), "pending CUDA error after begin capture");
+  rc = scc_solve_enqueue(c, d_labels);
+  cudaGraph_t graph = nullptr;
+  const cudaError_t ee = cudaStreamEndCapture(c->stream, &graph);
+  if (rc) {
+    if (graph) cudaGraphDestroy(graph);
+    return rc;
+  }
+  if (ee != cudaSuccess) return cuda_fail(ee, "end capture");
+  const cudaError_t ie = cudaGraphInstantiate(&c->solve_exec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (ie != cudaSuccess) {
+    c->solve_exec = nullptr;
+    return cuda_fail(ie, "instantiate captured solve");
+  }
+  return SCC_OK;
+}
+
+int scc_solve_replay(scc_ctx *c, uint32_t *nscc, scc_stats *st) {
+  sccb::clear_error();
+  if (!c || !c->solve_exec) return set_error(SCC_ERR_STATE, "no captured solve (call scc_solve_capture)");
+  int rc = use_device(c);
+  if (rc) return rc;
+  if (c->slot_dirty) {  // an earlier failure left election slots set: restore them outside the graph
+    CK(cudaMemsetAsync(c->slot.p, 0xff, c->slot.bytes, c->stream), "reset election slots");
+    c->slot_dirty = false;
+  }
+  CK(cudaEventRecord(c->ev0, c->stream), "event");  // ms_total: the whole replayed graph
+  CK(cudaGraphLaunch(c->solve_exec, c->stream), "graph launch");
+  CK(cudaEventRecord(c->ev1, c->stream), "event");
+  c->launches = 2;
+  return scc_solve_collect(c, nscc, st);
+}
+
+int scc_read_labels(scc_ctx *c, uint32_t *labels) {
+  sccb::clear_error();
+  int rc = need_graph(c);
+  if (rc) return rc;
+  if (!labels) return set_error(SCC_ERR_INVALID, "null output");
+  rc = use_device(c);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(labels, c->label.p, ((size_t)c->n + 1) * 4, cudaMemcpyDeviceToHost, c->stream), "labels D2H");
+  CK(cudaStreamSynchronize(c->stream), "labels D2H");
+  labels[0] = 0;
   return SCC_OK;
 }
 

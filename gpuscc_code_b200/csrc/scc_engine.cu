@@ -606,10 +606,12 @@ struct Eng {
       const unsigned long long ts = globaltimer_ns();
       uint32_t chg = 0;
       for_vertices([&](uint32_t v, bool valid) {
-        if (!list_mode) {  // whole warp = one bitmap word: skip words without a frontier vertex
-          const uint32_t w = v >> 5;
-          if ((ldm(vis + w) & ~ldm(exp + w) & ~ldm(P.s.elim + w)) == 0u) return;
-        }
+        // No warp-level "skip this word" shortcut here: visit bits change
+        // under other warps during the sweep, and lanes left diverged by the
+        // previous iteration's expansions read the word at different times,
+        // so such a test is not warp-uniform and would strand the lanes that
+        // enter the ballot below.  (The shortcuts in trim, pull, update and
+        // compaction test words only their own warp changes.)
         const bool fr = valid && live(v) && bit_test(vis, v) && !bit_test(exp, v);
         warp_set_bits(exp, v, fr, !list_mode);
         if (!fr) return;

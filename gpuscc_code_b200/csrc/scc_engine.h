@@ -149,6 +149,18 @@ cudaError_t launch_ranges(const Params &p, uint32_t *d_ranges, cudaStream_t stre
 cudaError_t check_device_csr(const uint32_t *off, const uint32_t *adj, uint32_t n, uint32_t m, uint32_t *d_bad,
                              uint32_t *h_bad, cudaStream_t st);
 
+}  // namespace sccb
+namespace sccg {
+struct BatchGraph;
+}
+namespace sccb {
+
+// Device build of a batch of independent graphs packed with global 1-based
+// ids (graph g owns a contiguous id range); arrays are cudaMalloc'ed.
+cudaError_t gen_batch_device(const sccg::BatchGraph *plan, uint32_t count, cudaStream_t st, uint32_t **d_off,
+                             uint32_t **d_adj, uint32_t **d_offT, uint32_t **d_adjT, uint32_t *n_out,
+                             uint32_t *m_out);
+
 // Device R-MAT build (scc_gen_device.cu); output arrays are cudaMalloc'ed.
 cudaError_t gen_rmat_device(uint32_t scale, uint64_t samples, uint32_t a_ppm, uint32_t b_ppm, uint32_t c_ppm,
                             uint64_t seed, int permute, cudaStream_t st, uint32_t **d_off, uint32_t **d_adj,

@@ -138,6 +138,31 @@ SCCG_HD uint32_t grid_edge(uint64_t seed, uint32_t side, uint64_t e, uint32_t bi
   return 1;
 }
 
+// One graph of a batch of independent graphs (see plan_batch in scc_host.cpp).
+struct BatchGraph {
+  uint32_t n;        // vertices
+  uint32_t type;     // 0 = Erdos-Renyi draws, 1 = R-MAT (0.57, 0.19, 0.19, 0.05)
+  uint32_t scale;    // ceil(log2 n) for R-MAT
+  uint32_t pad;
+  uint64_t samples;  // edge draws
+  uint64_t seed;
+};
+
+// Draw i of batch graph g: 0-based local (src, dst).  R-MAT draws over
+// 2^scale ids are permuted by the graph's bijection and folded into [0, n).
+SCCG_HD void batch_draw(const BatchGraph &g, uint64_t i, uint32_t &src, uint32_t &dst) {
+  if (g.type == 0) {
+    er_draw(g.seed, i, g.n, src, dst);
+    return;
+  }
+  const Rmat r = make_rmat(g.scale, 570000, 190000, 190000, g.seed);
+  const Perm p = make_perm(g.scale, g.seed);
+  uint32_t s, d;
+  r.draw(i, s, d);
+  src = p(s) % g.n;
+  dst = p(d) % g.n;
+}
+
 // Long-range edge k of the grid graph: uniform src, dst over side^2 vertices.
 SCCG_HD void grid_longrange(uint64_t seed, uint32_t nverts, uint64_t k, uint32_t &src, uint32_t &dst) {
   er_draw(seed ^ 0x4c4f4e47ull, k, nverts, src, dst);

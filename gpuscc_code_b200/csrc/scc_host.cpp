@@ -3,6 +3,7 @@
 #include <algorithm>
 #include <atomic>
 #include <chrono>
+#include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -127,6 +128,30 @@ int build_csr(uint32_t n, uint64_t ne, const uint32_t *src, const uint32_t *dst,
   if (!out->nodes || !out->edges || !out->nodesT || !out->edgesT) {
     scc_host_csr_free(out);
     return set_error(SCC_ERR_NOMEM, "host allocation of %u-vertex CSR failed", n);
+  }
+  return SCC_OK;
+}
+
+int plan_batch(uint32_t count, uint32_t n_lo, uint32_t n_hi, uint32_t deg_lo_milli, uint32_t deg_hi_milli,
+               uint64_t seed, std::vector<sccg::BatchGraph> *plan) {
+  if (count == 0 || n_lo < 2 || n_hi < n_lo || deg_hi_milli < deg_lo_milli)
+    return set_error(SCC_ERR_INVALID, "bad batch arguments");
+  plan->resize(count);
+  const double ln_lo = std::log((double)n_lo), ln_hi = std::log((double)n_hi);
+  for (uint32_t g = 0; g < count; ++g) {
+    const uint64_t h = sccg::mix64(seed ^ sccg::mix64((uint64_t)g ^ 0x4241544348ull));
+    const double u1 = (double)(h & 0xffffffffull) / 4294967296.0;
+    const double u2 = (double)((h >> 32) & 0x7fffffffull) / 2147483648.0;
+    sccg::BatchGraph b{};
+    uint32_t n = (uint32_t)std::floor(std::exp(ln_lo + u1 * (ln_hi - ln_lo)));
+    b.n = n < n_lo ? n_lo : (n > n_hi ? n_hi : n);
+    b.type = (uint32_t)(h >> 63);
+    b.scale = 1;
+    while ((1u << b.scale) < b.n) ++b.scale;
+    const double deg = (deg_lo_milli + u2 * (double)(deg_hi_milli - deg_lo_milli)) / 1000.0;
+    b.samples = (uint64_t)std::llround(deg * b.n);
+    b.seed = sccg::mix64(seed + g + 1);
+    (*plan)[g] = b;
   }
   return SCC_OK;
 }
@@ -336,6 +361,37 @@ int scc_gen_grid(uint32_t side, uint32_t bidir_ppm, uint32_t longrange_ppm, uint
     ++w;
   }
   return sccb::build_csr(n, w, src.data(), dst.data(), true, out);
+}
+
+int scc_gen_batch(uint32_t count, uint32_t n_lo, uint32_t n_hi, uint32_t deg_lo_milli, uint32_t deg_hi_milli,
+                  uint64_t seed, scc_host_csr *out, uint32_t *seg_first) {
+  sccb::clear_error();
+  if (!out || !seg_first) return set_error(SCC_ERR_INVALID, "null output");
+  std::vector<sccg::BatchGraph> plan;
+  int rc = sccb::plan_batch(count, n_lo, n_hi, deg_lo_milli, deg_hi_milli, seed, &plan);
+  if (rc) return rc;
+  std::vector<uint64_t> draw_base(count + 1, 0);
+  seg_first[0] = 1;
+  for (uint32_t g = 0; g < count; ++g) {
+    draw_base[g + 1] = draw_base[g] + plan[g].samples;
+    seg_first[g + 1] = seg_first[g] + plan[g].n;
+  }
+  const uint64_t total = draw_base[count];
+  const uint64_t n = (uint64_t)seg_first[count] - 1;
+  if (n >= (1u << 30)) return set_error(SCC_ERR_CAPACITY, "batch has %llu vertices", (unsigned long long)n);
+  std::vector<uint32_t> src(total), dst(total);
+  parallel_for(count, [&](uint64_t b, uint64_t e, unsigned) {
+    for (uint64_t g = b; g < e; ++g) {
+      const uint32_t base = seg_first[g];
+      for (uint64_t i = 0; i < plan[g].samples; ++i) {
+        uint32_t s, d;
+        sccg::batch_draw(plan[g], i, s, d);
+        src[draw_base[g] + i] = base + s;
+        dst[draw_base[g] + i] = base + d;
+      }
+    }
+  });
+  return sccb::build_csr((uint32_t)n, total, src.data(), dst.data(), true, out);
 }
 
 // ------------------------------------------------------------ -t Tarjan

@@ -15,3 +15,15 @@ void clear_error();
 int build_csr(uint32_t n, uint64_t ne, const uint32_t *src, const uint32_t *dst, bool drop_self, scc_host_csr *out);
 
 }  // namespace sccb
+#include <vector>
+
+#include "scc_gen.h"
+namespace sccb {
+
+// Per-graph parameters of a batch (deterministic in the arguments): type
+// ER / R-MAT 50/50, n log-uniform in [n_lo, n_hi], average out-degree
+// uniform in [deg_lo, deg_hi] (milli-units), per-graph seed.
+int plan_batch(uint32_t count, uint32_t n_lo, uint32_t n_hi, uint32_t deg_lo_milli, uint32_t deg_hi_milli,
+               uint64_t seed, std::vector<sccg::BatchGraph> *plan);
+
+}  // namespace sccb

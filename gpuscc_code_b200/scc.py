@@ -137,6 +137,20 @@ def gen_grid(side: int, bidir: float = 0.15, longrange: float = 0.001, seed: int
     return HostCSR(raw)
 
 
+BATCH_DEFAULTS = dict(n_lo=1000, n_hi=200_000, deg_lo=2.0, deg_hi=16.0)
+
+
+def gen_batch(count: int, n_lo: int = 1000, n_hi: int = 200_000, deg_lo: float = 2.0, deg_hi: float = 16.0,
+              seed: int = 4):
+    """`count` independent ER / R-MAT graphs packed into one CSR.
+    Returns (HostCSR, seg_first[count+1])."""
+    raw = scc_host_csr()
+    seg = np.zeros(count + 1, dtype=np.uint32)
+    check(lib.scc_gen_batch(count, n_lo, n_hi, int(round(deg_lo * 1000)), int(round(deg_hi * 1000)), seed,
+                            C.byref(raw), _ptr(seg)))
+    return HostCSR(raw), seg
+
+
 def tarjan(g: HostCSR):
     """tarjan.h:5 — the sequential CPU decomposition behind the apps' -t flag.
     Returns (labels[n+1], count, seconds)."""
@@ -238,6 +252,35 @@ class SCCContext:
                                       C.byref(d)))
         self.n = int(d.n)
         return d
+
+    def gen_batch_device(self, count: int, n_lo: int = 1000, n_hi: int = 200_000, deg_lo: float = 2.0,
+                         deg_hi: float = 16.0, seed: int = 4):
+        """Same batch as gen_batch, built on the device, bound with its segments.
+        Returns seg_first[count+1]."""
+        d = scc_dev_csr()
+        seg = np.zeros(count + 1, dtype=np.uint32)
+        check(lib.scc_gen_batch_device(self._h, count, n_lo, n_hi, int(round(deg_lo * 1000)),
+                                       int(round(deg_hi * 1000)), seed, C.byref(d), _ptr(seg)))
+        self.n = int(d.n)
+        self.m = int(d.m)
+        return seg
+
+    def capture(self, d_labels: int = 0):
+        """Capture the solve sequence into a CUDA graph (scc_solve_capture)."""
+        check(lib.scc_solve_capture(self._h, C.c_void_p(d_labels or None)))
+
+    def replay(self):
+        """Launch the captured solve -> (count, stats)."""
+        cnt = C.c_uint32()
+        st = scc_stats()
+        check(lib.scc_solve_replay(self._h, C.byref(cnt), C.byref(st)))
+        return int(cnt.value), st.as_dict()
+
+    def read_labels(self) -> np.ndarray:
+        """Labels of the last solve into the context's own buffer (host copy)."""
+        out = np.zeros(self.n + 1, dtype=np.uint32)
+        check(lib.scc_read_labels(self._h, _ptr(out)))
+        return out
 
     def download(self) -> HostCSR:
         raw = scc_host_csr()

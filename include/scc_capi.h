@@ -142,6 +142,15 @@ int scc_gen_er(uint32_t n, uint64_t samples, uint64_t seed, scc_host_csr *out);
 int scc_gen_grid(uint32_t side, uint32_t bidir_ppm, uint32_t longrange_ppm, uint64_t seed,
                  scc_host_csr *out);
 
+/* `count` independent graphs packed into one CSR (the batched workload):
+ * graph g is Erdos-Renyi or R-MAT (0.57, 0.19, 0.19, 0.05) with equal
+ * probability, n log-uniform in [n_lo, n_hi], average out-degree uniform in
+ * [deg_lo, deg_hi] (given in thousandths), self-loops dropped, duplicates
+ * merged; graph g owns the global ids seg_first[g] .. seg_first[g+1]-1
+ * (seg_first: count+1 entries, seg_first[0] = 1). */
+int scc_gen_batch(uint32_t count, uint32_t n_lo, uint32_t n_hi, uint32_t deg_lo_milli, uint32_t deg_hi_milli,
+                  uint64_t seed, scc_host_csr *out, uint32_t *seg_first);
+
 /* ---------------------------------------------------------- device graph */
 typedef struct scc_dev_csr {
   uint32_t n, m;
@@ -156,6 +165,11 @@ typedef struct scc_ctx scc_ctx;
 int scc_gen_rmat_device(scc_ctx *ctx, uint32_t scale, uint64_t samples, uint32_t a_ppm,
                         uint32_t b_ppm, uint32_t c_ppm, uint64_t seed, int permute,
                         scc_dev_csr *out);
+
+/* Same batch as scc_gen_batch, built on the device of `ctx`, bound as its
+ * graph with the segment table installed (seg_first: host, count+1). */
+int scc_gen_batch_device(scc_ctx *ctx, uint32_t count, uint32_t n_lo, uint32_t n_hi, uint32_t deg_lo_milli,
+                         uint32_t deg_hi_milli, uint64_t seed, scc_dev_csr *out, uint32_t *seg_first);
 
 /* --------------------------------------------------------------- context */
 int scc_ctx_create(int device, const scc_opts *opts, scc_ctx **out);
@@ -210,6 +224,16 @@ typedef struct scc_stats {
 int scc_solve(scc_ctx *ctx, uint32_t *labels, uint32_t *nscc, scc_stats *stats);
 /* Same, labels left in device memory (d_labels: device (n+1) or NULL). */
 int scc_solve_device(scc_ctx *ctx, uint32_t *d_labels, uint32_t *nscc, scc_stats *stats);
+/* Captures the enqueue sequence of scc_solve_enqueue (control reset, state
+ * init, the persistent cooperative launch) into a CUDA graph owned by the
+ * context, so repeated solves of the bound graph (e.g. a packed batch) are
+ * one graph launch each.  scc_solve_replay launches it and collects the
+ * result like scc_solve_collect.  Re-capture after binding another graph. */
+int scc_solve_capture(scc_ctx *ctx, uint32_t *d_labels);
+int scc_solve_replay(scc_ctx *ctx, uint32_t *nscc, scc_stats *stats);
+/* Copy the labels of the last solve that wrote the context's own label
+ * buffer (d_labels = NULL) to the host: labels (n+1). */
+int scc_read_labels(scc_ctx *ctx, uint32_t *labels);
 /* No counterpart in the reference (it cudaMallocs everything per call).
  * The whole decomposition for callers that cannot allocate device memory —
  * code running while a stream is captured, plugins whose host framework owns

@@ -86,6 +86,16 @@ def test_option_space(ctx, opts):
         assert np.array_equal(labels, ref), name
 
 
+@pytest.mark.parametrize("alg", ARMS)
+def test_graphs_needing_several_sweep_iterations_per_cta(ctx, alg):
+    """More vertices than threads in the persistent grid (148 SMs x 1024),
+    so every full-id sweep runs several grid-stride iterations per CTA."""
+    for g in (scc.gen_rmat(18, 4 << 18, seed=3), scc.gen_er(300_000, 450_000, seed=8)):
+        ref, rcnt = oracle_labels(g)
+        labels, cnt, _ = solve(ctx, g, alg=alg, wcc=True, trim2=True)
+        assert cnt == rcnt and np.array_equal(labels, ref)
+
+
 def test_config1_rmat16(ctx):
     """R-MAT 2^16 vertices, 2^20 samples, (0.57, 0.19, 0.19, 0.05), seed 1."""
     g = scc.gen_rmat(16, 1 << 20, seed=1)
