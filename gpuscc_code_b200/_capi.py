@@ -69,6 +69,32 @@ class scc_stats(C.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_ if name != "reserved"}
 
 
+class scc_server_cfg(C.Structure):
+    _fields_ = [
+        ("device", C.c_int32), ("batching", C.c_int32), ("max_batch_graphs", C.c_uint32),
+        ("max_batch_vertices", C.c_uint32), ("max_batch_edges", C.c_uint32), ("pad", C.c_uint32),
+        ("mem_budget", C.c_uint64), ("opts", scc_opts),
+    ]
+
+
+class scc_request_info(C.Structure):
+    _fields_ = [
+        ("nscc", C.c_uint32), ("batch_graphs", C.c_uint32), ("choice", C.c_int32 * 3), ("status", C.c_int32),
+        ("queue_ms", C.c_double), ("latency_ms", C.c_double), ("solve_ms", C.c_double),
+    ]
+
+
+class scc_server_stats(C.Structure):
+    _fields_ = [(k, C.c_uint64) for k in ("submitted", "completed", "rejected", "batches", "graphs_batched",
+                                           "resident_bytes", "peak_resident_bytes", "budget_bytes")]
+
+    def as_dict(self) -> dict:
+        return {name: int(getattr(self, name)) for name, _ in self._fields_}
+
+
+f32p = C.POINTER(C.c_float)
+i32p = C.POINTER(C.c_int32)
+
 # (name, restype, argtypes) for every symbol include/scc_capi.h declares
 SIGNATURES = [
     ("scc_last_error", C.c_char_p, []),
@@ -121,6 +147,26 @@ SIGNATURES = [
     ("scc_get_states", C.c_int, [C.c_void_p, C.POINTER(C.c_uint8)]),
     ("scc_get_ranges", C.c_int, [C.c_void_p, u32p]),
     ("scc_get_labels", C.c_int, [C.c_void_p, u32p, u32p]),
+    ("scc_graph_features", C.c_int, [C.c_void_p, f32p]),
+    ("scc_mlp_create", C.c_int, [C.c_int, C.c_uint64, C.POINTER(C.c_void_p)]),
+    ("scc_mlp_destroy", C.c_int, [C.c_void_p]),
+    ("scc_mlp_param_count", C.c_uint32, []),
+    ("scc_mlp_params", C.c_int, [C.c_void_p, f32p, C.c_int]),
+    ("scc_mlp_norm", C.c_int, [C.c_void_p, f32p, f32p, C.c_int]),
+    ("scc_mlp_forward", C.c_int, [C.c_void_p, f32p, C.c_uint32, f32p]),
+    ("scc_mlp_loss_grad", C.c_int, [C.c_void_p, f32p, i32p, C.c_uint32, f32p, f32p]),
+    ("scc_mlp_train", C.c_int, [C.c_void_p, f32p, i32p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_float,
+                                C.c_uint64, f32p]),
+    ("scc_mlp_predict", C.c_int, [C.c_void_p, f32p, C.c_uint32, i32p]),
+    ("scc_mlp_apply", C.c_int, [i32p, C.POINTER(scc_opts)]),
+    ("scc_server_cfg_default", None, [C.POINTER(scc_server_cfg)]),
+    ("scc_server_start", C.c_int, [C.POINTER(scc_server_cfg), C.POINTER(C.c_void_p)]),
+    ("scc_server_set_model", C.c_int, [C.c_void_p, f32p, f32p, f32p]),
+    ("scc_server_submit", C.c_int, [C.c_void_p, C.POINTER(scc_host_csr), u32p, C.POINTER(C.c_uint64)]),
+    ("scc_server_poll", C.c_int, [C.c_void_p, C.c_uint64, C.POINTER(scc_request_info)]),
+    ("scc_server_wait", C.c_int, [C.c_void_p, C.c_uint64, C.c_uint32, C.POINTER(scc_request_info)]),
+    ("scc_server_get_stats", C.c_int, [C.c_void_p, C.POINTER(scc_server_stats)]),
+    ("scc_server_stop", C.c_int, [C.c_void_p]),
 ]
 
 

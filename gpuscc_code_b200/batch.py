@@ -104,3 +104,27 @@ def solve_each(graphs: list[HostCSR], ctx: SCCContext):
         out.append((labels, cnt))
         ms += st["ms_total"]
     return out, ms
+
+
+def shard_graphs(weights, world: int) -> list[list[int]]:
+    """Independent graphs over `world` ranks (one GPU each): longest-processing-
+    time greedy on the weights (edge bytes), heaviest first, each to the
+    least-loaded rank (ties to the lower rank).  Deterministic, so every rank
+    computes the same plan without exchanging it; graph order is kept inside
+    a shard.  No graph crosses ranks, so the solves need no collective."""
+    if world < 1:
+        raise ValueError("world must be >= 1")
+    w = np.asarray(weights, dtype=np.float64)
+    order = sorted(range(len(w)), key=lambda i: (-w[i], i))
+    load = [0.0] * world
+    shards: list[list[int]] = [[] for _ in range(world)]
+    for i in order:
+        r = min(range(world), key=lambda k: (load[k], k))
+        shards[r].append(i)
+        load[r] += w[i]
+    return [sorted(s) for s in shards]
+
+
+def graph_weight(n: int, m: int) -> int:
+    """Bytes the solve of one graph must touch (CSR + transpose + labels)."""
+    return 8 * (n + 1) + 8 * m + 4 * n

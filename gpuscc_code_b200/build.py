@@ -23,9 +23,9 @@ CUDA_HOME = Path(os.environ.get("CUDA_HOME", "/usr/local/cuda"))
 NVCC = str(CUDA_HOME / "bin" / "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
-CU_SOURCES = ["scc_engine.cu", "scc_gen_device.cu", "scc_noalloc.cu"]
+CU_SOURCES = ["scc_engine.cu", "scc_gen_device.cu", "scc_noalloc.cu", "scc_features.cu", "scc_mlp.cu", "scc_server.cu"]
 CPP_SOURCES = ["scc_capi.cpp", "scc_host.cpp"]
-HEADERS = ["scc_device.cuh", "scc_engine.h", "scc_gen.h", "scc_internal.h"]
+HEADERS = ["scc_device.cuh", "scc_engine.h", "scc_gen.h", "scc_internal.h", "scc_features.h"]
 APPS = {"scc": [], "scc_w": ["-DSCC_APP_WCC"], "scc_2_w": ["-DSCC_APP_WCC", "-DSCC_APP_TRIM2"]}
 
 

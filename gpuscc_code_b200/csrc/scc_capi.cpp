@@ -11,6 +11,7 @@
 
 #include "scc_capi.h"
 #include "scc_engine.h"
+#include "scc_features.h"
 #include "scc_internal.h"
 
 namespace sccb {
@@ -72,6 +73,7 @@ struct scc_ctx {
   uint32_t cap_n = 0, cap_h = 0;
   bool have_state = false;
   DBuf label, range, rpivot, aux, bitmaps, qa, qb, act0, act1, piv, pivkey, slot, heavy, ctl, seg;
+  DBuf feat;  // scratch of scc_graph_features
   uint32_t nwords = 0;
   bool slot_dirty = true;
   uint32_t nseg = 0;
@@ -353,7 +355,7 @@ int scc_ctx_destroy(scc_ctx *c) {
   if (c->stream) cudaStreamSynchronize(c->stream);
   for (DBuf *b : {&c->g_off, &c->g_adj, &c->g_offT, &c->g_adjT, &c->label, &c->range, &c->rpivot, &c->aux,
                   &c->bitmaps, &c->qa, &c->qb, &c->act0, &c->act1, &c->piv, &c->pivkey, &c->slot, &c->heavy,
-                  &c->ctl, &c->seg})
+                  &c->ctl, &c->seg, &c->feat})
     b->release();
   if (c->h_ctl) cudaFreeHost(c->h_ctl);
   if (c->ev0) cudaEventDestroy(c->ev0);
@@ -877,6 +879,25 @@ int scc_get_ranges(scc_ctx *c, uint32_t *ranges) {
   if (e != cudaSuccess) return cuda_fail(e, "ranges export");
   return SCC_OK;
 }
+int scc_graph_features(scc_ctx *c, float *feat) {
+  sccb::clear_error();
+  if (!c || !feat) return set_error(SCC_ERR_INVALID, "null argument");
+  int rc = use_device(c);
+  if (!rc) rc = need_graph(c);
+  if (rc) return rc;
+  CK(c->feat.ensure(sccb::features_scratch_bytes(c->n)), "alloc feature scratch");
+  sccb::EngGraph g{};
+  g.n = c->n;
+  g.m = c->m;
+  g.sorted_unique = c->sorted_unique ? 1u : 0u;
+  g.off = c->d_off;
+  g.adj = c->d_adj;
+  g.offT = c->d_offT;
+  g.adjT = c->d_adjT;
+  CK(sccb::graph_features(g, c->feat.p, c->feat.bytes, feat, c->stream), "graph features");
+  return SCC_OK;
+}
+
 int scc_get_labels(scc_ctx *c, uint32_t *labels, uint32_t *nscc) {
   int rc = run_phase(c, sccb::PH_FINALIZE);
   if (rc) return rc;

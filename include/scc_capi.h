@@ -303,6 +303,99 @@ int scc_get_ranges(scc_ctx *ctx, uint32_t *ranges);
  * Fails with SCC_ERR_STATE while active vertices remain. */
 int scc_get_labels(scc_ctx *ctx, uint32_t *labels, uint32_t *nscc);
 
+/* ------------------------------------------------------ strategy network
+ * No counterpart in the reference (its strategy is fixed by -a).  A 3-layer
+ * fp32 MLP, 16 -> 64 -> 64 -> 8 with ReLU, whose three softmax heads pick,
+ * per graph, options that never change the labels:
+ *   head 0 (2 classes): pivot_rule  {MIN_ID, MAX_DEGREE}
+ *   head 1 (2 classes): trim_depth  {0 = to fixpoint, 1 = one iteration}
+ *   head 2 (4 classes): reach arm / switch point
+ *                       {h at 10 permille, h at 100, h at 1000, c at 10}
+ * Choice (0,0,0) is the plain hybrid (-a h, reference switch n/100). */
+#define SCC_FEATURES 16
+#define SCC_MLP_HEADS 3
+#define SCC_MLP_OUTPUTS 8
+/* Statistics of the bound graph, computed on the device (see the feature
+ * list in scc_features.h): feat receives 16 floats. */
+int scc_graph_features(scc_ctx *ctx, float *feat);
+typedef struct scc_mlp scc_mlp;
+/* Parameters He-uniform from seed, biases 0, normalisation mean 0 / scale 1. */
+int scc_mlp_create(int device, uint64_t seed, scc_mlp **out);
+int scc_mlp_destroy(scc_mlp *m);
+/* Number of floats in the flat parameter vector: W1[16][64], b1[64],
+ * W2[64][64], b2[64], W3[64][8], b3[8] (row = input unit). */
+uint32_t scc_mlp_param_count(void);
+/* get != 0: copy the parameters to buf; else load them from buf (and reset
+ * the optimiser state). */
+int scc_mlp_params(scc_mlp *m, float *buf, int get);
+/* Input normalisation applied inside the forward pass: x' = (x - mean) * scale
+ * (16 floats each); get != 0 reads it back. */
+int scc_mlp_norm(scc_mlp *m, float *mean, float *scale, int get);
+/* logits: B x 8 (head 0 in [0,2), head 1 in [2,4), head 2 in [4,8)). */
+int scc_mlp_forward(scc_mlp *m, const float *x, uint32_t B, float *logits);
+/* Mean over the B samples of the summed per-head cross-entropy (y: B x 3
+ * class indices) and its gradient w.r.t. the flat parameters (either
+ * output may be NULL). */
+int scc_mlp_loss_grad(scc_mlp *m, const float *x, const int32_t *y, uint32_t B, float *loss, float *grad);
+/* Adam (beta 0.9/0.999, eps 1e-8) over seeded shuffled minibatches, all on
+ * the device; final_loss = loss of the last minibatch. */
+int scc_mlp_train(scc_mlp *m, const float *x, const int32_t *y, uint32_t B, uint32_t epochs, uint32_t batch,
+                  float lr, uint64_t seed, float *final_loss);
+/* Arg-max class of each head: choice B x 3. */
+int scc_mlp_predict(scc_mlp *m, const float *x, uint32_t B, int32_t *choice);
+/* Writes the options a choice stands for into opts (other fields kept). */
+int scc_mlp_apply(const int32_t *choice, scc_opts *opts);
+
+/* ---------------------------------------------------------------- server
+ * No counterpart in the reference.  A request loop on one device: graphs
+ * are admitted while their CSR fits in the memory budget (FIFO), uploaded
+ * on a copy stream while earlier work runs, kept resident, and solved in
+ * batches of the requests that are ready when the device frees up (one
+ * segmented persistent launch per batch; a graph alone is bound in place).
+ * With a strategy network loaded, each request's options come from it and
+ * only requests with the same options share a batch. */
+typedef struct scc_server scc_server;
+typedef struct scc_server_cfg {
+  int32_t device;
+  int32_t batching;            /* 0: one graph per launch, in arrival order */
+  uint32_t max_batch_graphs;   /* 0 = 256 */
+  uint32_t max_batch_vertices; /* capacity of the packed batch CSR (0 = 1<<24) */
+  uint32_t max_batch_edges;    /* (0 = 1<<27) */
+  uint32_t pad;
+  uint64_t mem_budget;         /* device bytes for resident request graphs (0 = half the free memory) */
+  scc_opts opts;               /* options of the plain method (and the base the network edits) */
+} scc_server_cfg;
+typedef struct scc_request_info {
+  uint32_t nscc;
+  uint32_t batch_graphs;       /* requests solved in the same launch */
+  int32_t choice[3];           /* options picked (all 0 without a network) */
+  int32_t status;              /* SCC_OK or the solve's error code */
+  double queue_ms;             /* submit -> upload started (waiting for memory) */
+  double latency_ms;           /* submit -> labels on the host */
+  double solve_ms;             /* device time of the batch's solve */
+} scc_request_info;
+typedef struct scc_server_stats {
+  uint64_t submitted, completed, rejected, batches, graphs_batched;
+  uint64_t resident_bytes, peak_resident_bytes, budget_bytes;
+} scc_server_stats;
+void scc_server_cfg_default(scc_server_cfg *cfg);
+int scc_server_start(const scc_server_cfg *cfg, scc_server **out);
+/* Load a strategy network (flat parameters and normalisation as in
+ * scc_mlp_params / scc_mlp_norm); NULL params unloads it. */
+int scc_server_set_model(scc_server *s, const float *params, const float *mean, const float *scale);
+/* Queue a graph.  g's arrays and labels (host, n+1) must stay valid until
+ * the request completes.  SCC_ERR_REJECTED if the graph alone exceeds the
+ * memory budget. */
+int scc_server_submit(scc_server *s, const scc_host_csr *g, uint32_t *labels, uint64_t *id);
+/* SCC_ERR_BUSY while the request runs; otherwise its info, and the request
+ * is retired.  A failed solve returns its error code (info->status). */
+int scc_server_poll(scc_server *s, uint64_t id, scc_request_info *info);
+/* Like poll but blocks up to timeout_ms (0 = no limit). */
+int scc_server_wait(scc_server *s, uint64_t id, uint32_t timeout_ms, scc_request_info *info);
+int scc_server_get_stats(scc_server *s, scc_server_stats *st);
+/* Finishes the queued requests, then stops. */
+int scc_server_stop(scc_server *s);
+
 #ifdef __cplusplus
 }
 #endif
