@@ -452,6 +452,79 @@ def run_batch(args) -> None:
     ctx.close()
 
 
+def run_serve(args) -> None:
+    """Served stream: Poisson arrivals of R-MAT (scale 14-22, average degree
+    8-32) and grid graphs (side 256-2048, 10-30 % bidirectional), seed 5.
+    A pool of distinct graphs is generated first and the stream cycles
+    through it.  Three arms serve the same arrival sequence: the plain
+    hybrid one graph per launch, continuous batching, and continuous batching
+    with the trained strategy network.  Every request's labels are compared
+    with the same graph solved alone by the plain method."""
+    import numpy as np
+    import torch
+
+    import gpuscc_code_b200 as scc
+    from gpuscc_code_b200 import learned
+    from gpuscc_code_b200.serve import Server, make_graph, poisson_arrivals, run_stream, stream_spec
+
+    torch.cuda.set_device(0)
+    base = scc.Options(alg="h", wcc=True, trim2=True)
+    ctx = scc.SCCContext(0, base)
+    pool = [make_graph(stream_spec(i, seed=5), ctx) for i in range(args.serve_pool)]
+    # alone: plain method, one graph at a time (also the labels every arm must reproduce)
+    alone, svc_ms = [], []
+    for g in pool:
+        ctx.upload(g)
+        labels, cnt, st = ctx.solve()
+        alone.append(labels.copy())
+        svc_ms.append(st["ms_total"])
+    ctx.close()
+    reqs = [pool[i % len(pool)] for i in range(args.serve_requests)]
+    ref = [alone[i % len(pool)] for i in range(args.serve_requests)]
+    rate = args.serve_rate
+    if rate <= 0:  # load the plain server close to its device capacity
+        rate = 0.9 * 1e3 / float(np.mean(svc_ms))
+    arrivals = poisson_arrivals(len(reqs), rate, seed=5)
+    model = learned.DEFAULT_MODEL if learned.DEFAULT_MODEL.exists() else None
+    arms = [("plain", dict(batching=False), None), ("batched", dict(batching=True), None)]
+    if model is not None:
+        arms.append(("batched_learned", dict(batching=True), model))
+    out = {}
+    for name, kw, mdl in arms:
+        with Server(0, base, model=mdl, **kw) as srv:
+            run_stream(srv, reqs[:min(8, len(reqs))], np.zeros(min(8, len(reqs))))  # warm-up
+            res = run_stream(srv, reqs, arrivals)
+            st = srv.stats()
+        exact = all(np.array_equal(a, b) for a, b in zip(res["labels"], ref))
+        if not exact:
+            raise SystemExit(f"serve arm {name}: labels differ from the graph solved alone")
+        picks = {}
+        for info in res["info"]:
+            picks[str(info["choice"])] = picks.get(str(info["choice"]), 0) + 1
+        out[name] = {"graphs_per_s": res["graphs_per_s"], "p50_ms": res["p50_ms"], "p99_ms": res["p99_ms"],
+                     "mean_batch": float(np.mean([i["batch_graphs"] for i in res["info"]])),
+                     "batches": st["batches"] - 1 if st["batches"] else 0, "labels_exact": exact,
+                     "peak_resident_bytes": st["peak_resident_bytes"], "choices": picks}
+        del res
+    best = out.get("batched_learned", out["batched"])
+    n_tot = sum(int(g.n) for g in reqs)
+    m_tot = sum(int(g.m) for g in reqs)
+    line = {
+        "metric": "served SCC graphs/s (Poisson stream of R-MAT + grid graphs, p50/p99 latency)",
+        "value": best["graphs_per_s"], "unit": "graphs/s", "n_gpus": 1, "steps": 1, "warmup": 1,
+        "ms_per_step": 1e3 * len(reqs) / best["graphs_per_s"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u32", "data": "synthetic (stream generated in-process, seed 5)",
+        "config": {"workload": f"serve{len(reqs)}_pool{len(pool)}_rmat14-22_grid256-2048",
+                   "requests": len(reqs), "distinct_graphs": len(pool), "rate_per_s": rate,
+                   "vertices": n_tot, "edges": m_tot, "model": str(model.name) if model else None},
+        "arms": out,
+        "speedup_vs_plain": {k: v["graphs_per_s"] / out["plain"]["graphs_per_s"] for k, v in out.items()},
+        "p99_vs_plain": {k: out["plain"]["p99_ms"] / v["p99_ms"] for k, v in out.items()},
+        "plain_mean_service_ms": float(np.mean(svc_ms)),
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -469,18 +542,24 @@ def main():
     ap.add_argument("--trace", action="store_true", help="include the per-sweep device trace in the line")
     ap.add_argument("--opt", action="append", default=[], metavar="KEY=VALUE",
                     help="override an engine option (scc_opts field), e.g. --opt occupancy=3")
-    ap.add_argument("--workload", choices=["rmat26", "batch"], default="rmat26",
-                    help="rmat26: the headline line; batch: 4096 packed graphs in one launch vs one launch each")
+    ap.add_argument("--workload", choices=["rmat26", "batch", "serve"], default="rmat26",
+                    help="rmat26: the headline line; batch: 4096 packed graphs in one launch vs one launch each; "
+                         "serve: Poisson stream through the request loop (plain / batched / batched + network)")
+    ap.add_argument("--serve-pool", type=int, default=48, help="serve: distinct graphs in the stream")
+    ap.add_argument("--serve-requests", type=int, default=240, help="serve: requests in the stream")
+    ap.add_argument("--serve-rate", type=float, default=0.0,
+                    help="serve: arrivals per second (0 = 0.9 x the plain method's device throughput)")
     ap.add_argument("--batch-count", type=int, default=4096)
     ap.add_argument("--no-tune", action="store_true", help="batch: skip the autotuner")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
-    if args.workload == "batch":
+    if args.workload in ("batch", "serve"):
         if args.impl == "reference":
-            print(json.dumps({"impl": "reference", "unavailable": "the batched workload has no reference path"}))
+            print(json.dumps({"impl": "reference",
+                              "unavailable": f"the {args.workload} workload has no reference path"}))
             return
-        run_batch(args)
+        run_batch(args) if args.workload == "batch" else run_serve(args)
     elif args.impl == "reference":
         run_reference(args)
     else:

@@ -151,3 +151,15 @@ def test_shard_plan_partitions_and_balances():
         assert flat == list(range(101))
         loads = [w[s].sum() for s in shards]
         assert max(loads) - min(loads) <= w.max()
+
+
+def test_no_cpu_fallback_without_a_device():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a CUDA device is present")
+    with pytest.raises(scc.SCCError) as ei:
+        scc.SCCContext(0)
+    assert ei.value.code == _capi.SCC_ERR_NODEVICE
+    with pytest.raises(scc.SCCError):
+        from gpuscc_code_b200.serve import Server
+        Server(0)
