@@ -186,9 +186,13 @@ def run_reference(args) -> None:
     import gpuscc_code_b200 as scc
 
     scale = args.ref_scale
-    with scc.SCCContext(0) as ctx:
-        ctx.gen_rmat_device(scale, 16 << scale, ABC, args.seed)
-        g = ctx.download()
+    grid = args.workload == "grid"
+    if grid:
+        g = scc.gen_grid(args.grid_side, 0.15, 0.001, seed=3)
+    else:
+        with scc.SCCContext(0) as ctx:
+            ctx.gen_rmat_device(scale, 16 << scale, ABC, args.seed)
+            g = ctx.download()
     kind = "reference" if oracle.ref_lib() is not None else "port"
     times = []
     restore = quiet_stdout()
@@ -207,8 +211,12 @@ def run_reference(args) -> None:
     value = g.m / per
     sample = (f"R-MAT scale {scale}, 2^{scale + 4} samples (same generator, (a,b,c,d), permutation, seed "
               f"{args.seed}): n={g.n}, m={g.m}; one decomposition per step")
+    metric = METRIC
+    if grid:
+        sample = f"the whole {args.grid_side}^2 grid graph (n={g.n}, m={g.m}); one decomposition per step"
+        metric = f"SCC edges/s ({args.grid_side}x{args.grid_side} grid, 15% bidirectional, scc_2_w -a h, 1 B200)"
     line = {
-        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "impl": "reference", "metric": metric, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": per * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
         "config": workload_config(args.scale, args.samples_log2, args.seed,
@@ -242,8 +250,17 @@ def run_ours(args) -> None:
         overrides[k] = v if k == "alg" else int(v)
     opts = scc.Options(**{"alg": "h", "wcc": True, "trim2": True, **overrides})
     ctx = scc.SCCContext(local, opts)
-    d = ctx.gen_rmat_device(scale, samples, ABC, args.seed)
-    n, m = int(d.n), int(d.m)
+    grid = args.workload == "grid"
+    if grid:
+        # 4096 x 4096 grid, every grid edge oriented by a coin flip, 15 % kept in
+        # both directions, plus random long-range edges numbering 0.1 % of the
+        # grid edges, seed 3 (host generator, then uploaded)
+        gh = scc.gen_grid(args.grid_side, 0.15, 0.001, seed=3)
+        ctx.upload(gh)
+        n, m = int(gh.n), int(gh.m)
+    else:
+        d = ctx.gen_rmat_device(scale, samples, ABC, args.seed)
+        n, m = int(d.n), int(d.m)
     stream = torch.cuda.ExternalStream(ctx.stream)
     d_labels = torch.zeros(n + 1, dtype=torch.int32, device=f"cuda:{local}")
 
@@ -292,7 +309,7 @@ def run_ours(args) -> None:
     achieved = b_alg(n, m) / (kern_ms / 1e3) / 1e9
     traffic = None
     prof = ROOT / "profiles" / "traffic_rmat_scc_2_w.json"
-    if prof.exists():
+    if prof.exists() and not grid:
         try:
             t = json.loads(prof.read_text())
             traffic = float(t["bytes_per_edge"]) * m + float(t.get("bytes_per_vertex", 0.0)) * n
@@ -330,7 +347,24 @@ def run_ours(args) -> None:
                "d2h_bytes_per_step": 4 * (n + 1), "ms_per_step": e2e_s * 1e3, "steps": e2e_steps}
 
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu:
+    if rank == 0 and world == 1 and not args.no_cpu and grid:
+        import oracle
+        kind = "reference" if oracle.ref_lib() is not None else "port"
+        restore = quiet_stdout()
+        try:
+            t0 = time.perf_counter()
+            if kind == "reference":
+                oracle.ref_tarjan(gh.n, gh.nodes, gh.edges)
+            else:
+                oracle.tarjan_labels(gh.n, gh.nodes, gh.edges)
+            secs = time.perf_counter() - t0
+        finally:
+            restore()
+        cpu = {"value": m / secs, "unit": UNIT, "cores": 1, "kind": kind, "host_cores_available": os.cpu_count(),
+               "sample": f"the whole grid graph (n={n}, m={m}); "
+                         f"{'tarjan.cpp TR_Decomposition' if kind == 'reference' else 'oracle port'} on 1 host "
+                         f"thread, wall {secs:.2f} s"}
+    elif rank == 0 and world == 1 and not args.no_cpu:
         rate, kind, sample, _ = cpu_tarjan_rate(args.cpu_scale, args.seed, local)
         cpu = {"value": rate, "unit": UNIT, "cores": 1, "kind": kind, "sample": sample,
                "host_cores_available": os.cpu_count()}
@@ -340,13 +374,25 @@ def run_ours(args) -> None:
     if rank != 0:
         ctx.close()
         return
+    if grid:
+        metric = f"SCC edges/s ({args.grid_side}x{args.grid_side} grid, 15% bidirectional, scc_2_w -a {opts.alg}, 1 B200)"
+        data = "synthetic (grid generated on the host, seed 3)"
+        config = {"workload": f"grid{args.grid_side}_bidir15_lr0.1_scc_2_w", "n": n, "m": m, "nscc": cnt,
+                  "graph": f"{args.grid_side}^2 grid, edges oriented at random, 15% bidirectional, long-range "
+                           "edges = 0.1% of grid edges, seed 3",
+                  "index_dtype": "u32", "l2": "inputs larger than L2 (CSR + transpose ~0.4 GB); no flush",
+                  "parallelism": f"replicas{world}", "engine_overrides": overrides,
+                  "rounds": st.get("steps")}
+    else:
+        metric, data = METRIC, "synthetic (R-MAT generated on the device, seed 2)"
+        config = workload_config(scale, args.samples_log2, args.seed,
+                                 {"n": n, "m": m, "nscc": cnt, "parallelism": f"replicas{world}",
+                                  "engine_overrides": overrides})
     line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "metric": metric, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "u32", "data": "synthetic (R-MAT generated on the device, seed 2)",
-        "config": workload_config(scale, args.samples_log2, args.seed,
-                                  {"n": n, "m": m, "nscc": cnt, "parallelism": f"replicas{world}",
-                                   "engine_overrides": overrides}),
+        "vs_baseline": None, "dtype": "u32", "data": data,
+        "config": config,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
                      "kernel": "scc_persistent<256> (+ per-step init pass)", "kernel_ms": kern_ms,
@@ -542,9 +588,11 @@ def main():
     ap.add_argument("--trace", action="store_true", help="include the per-sweep device trace in the line")
     ap.add_argument("--opt", action="append", default=[], metavar="KEY=VALUE",
                     help="override an engine option (scc_opts field), e.g. --opt occupancy=3")
-    ap.add_argument("--workload", choices=["rmat26", "batch", "serve"], default="rmat26",
+    ap.add_argument("--grid-side", type=int, default=4096, help="grid: side of the grid graph")
+    ap.add_argument("--workload", choices=["rmat26", "grid", "batch", "serve"], default="rmat26",
                     help="rmat26: the headline line; batch: 4096 packed graphs in one launch vs one launch each; "
-                         "serve: Poisson stream through the request loop (plain / batched / batched + network)")
+                         "serve: Poisson stream through the request loop (plain / batched / batched + network); "
+                         "grid: the 4096^2 high-diameter grid graph")
     ap.add_argument("--serve-pool", type=int, default=48, help="serve: distinct graphs in the stream")
     ap.add_argument("--serve-requests", type=int, default=240, help="serve: requests in the stream")
     ap.add_argument("--serve-rate", type=float, default=0.0,

@@ -148,7 +148,32 @@ struct Eng {
   template <class L, class F>
   __device__ void for_vertices_pf(L &&load, F &&f) {
     if (list_mode) {
-      for_vertices([&](uint32_t v, bool valid) { f(v, valid, load(v, valid)); });
+      // two-deep: the list entry two iterations ahead and the per-vertex
+      // loads of the next entry are in flight while f runs on the current one
+      const uint32_t *lst = P.s.act[act_sel];
+      const uint32_t cnt = act_count;
+      const uint32_t lim = (cnt + BS - 1u) / BS * BS;
+      const uint32_t stride = gstride();
+      uint32_t base = blockIdx.x * BS;
+      if (base >= lim) return;
+      const uint32_t i0 = base + threadIdx.x, i1 = i0 + stride;
+      bool val0 = i0 < cnt, val1 = i1 < cnt;
+      uint32_t v0 = val0 ? ldm(lst + i0) : 0u;
+      uint32_t v1 = val1 ? ldm(lst + i1) : 0u;
+      auto pre = load(v0, val0);
+      for (; base < lim; base += stride) {
+        const uint32_t i2 = base + 2u * stride + threadIdx.x;
+        const bool val2 = i2 < cnt;
+        const uint32_t v2 = val2 ? ldm(lst + i2) : 0u;
+        auto nxt = pre;
+        if (base + stride < lim) nxt = load(v1, val1);
+        f(v0, val0, pre);
+        pre = nxt;
+        v0 = v1;
+        val0 = val1;
+        v1 = v2;
+        val1 = val2;
+      }
       return;
     }
     const uint32_t lim = P.s.nwords * 32u;
@@ -295,8 +320,9 @@ struct Eng {
           best = key < best ? key : best;
         }
       }
-      // neighbours can only lose their last partner if v has edges at all
-      const bool q = t && (a1 != a0 || b1 != b0);
+      // neighbours can only lose their last partner if v has edges at all;
+      // a single-iteration trim never reads the queue
+      const bool q = max_it > 1 && t && (a1 != a0 || b1 != b0);
       warp_set_bits(s.tflag, v, t, !list_mode);
       warp_set_bits(s.elim, v, t, !list_mode);
       stage_put(tq, q, v);
@@ -973,10 +999,11 @@ struct Eng {
     refresh_mode();
   }
 
-  __device__ void maybe_compact() {
+  // compacts when fewer than span / ratio vertices are live
+  __device__ void maybe_compact(uint32_t ratio = 4) {
     const uint32_t nlive = ldm(&c->n_live);
     const uint32_t span = list_mode ? act_count : P.g.n;
-    if (nlive > 0 && (unsigned long long)nlive * 4ull < span) compact();
+    if (nlive > 0 && (unsigned long long)nlive * ratio < span) compact();
   }
 
   __device__ void sync_live() {
@@ -1061,6 +1088,11 @@ struct Eng {
       // The first round's trim would run on the same live set and partition;
       // what it could still remove, later partition-aware trims remove.
       trim_fresh = true;
+      // power-law graphs lose most vertices to the first trim: sweep the
+      // survivors' list from the first round on
+      const unsigned long long tc = globaltimer_ns();
+      maybe_compact(2);
+      prof(PR_COMPACT, tc);
     }
     timed(c->ns_trim, t0);
     t0 = globaltimer_ns();

@@ -163,3 +163,23 @@ def test_no_cpu_fallback_without_a_device():
     with pytest.raises(scc.SCCError):
         from gpuscc_code_b200.serve import Server
         Server(0)
+
+
+def test_trace_labels_and_pick_times():
+    from gpuscc_code_b200 import learned
+    assert len(learned.CHOICES) == 16 and learned.CHOICES[0] == learned.PLAIN
+    T = np.full((3, 16), 10.0)
+    T[0, 5] = 1.0
+    T[1, 0] = 2.0
+    T[2, 15] = 3.0
+    y = learned.labels_from_times(T)
+    assert [tuple(r) for r in y] == [learned.CHOICES[5], learned.CHOICES[0], learned.CHOICES[15]]
+    assert learned.choice_times(T, y).tolist() == [1.0, 2.0, 3.0]
+
+
+def test_apply_choice_keeps_base_options():
+    from gpuscc_code_b200 import learned
+    base = scc.Options(alg="h", wcc=True, trim2=True, heavy_degree=1024)
+    o = learned.apply_choice((1, 1, 3), base)
+    assert o.alg == "c" and o.pivot_rule == 1 and o.trim_depth == 1 and o.switch_permille == 10
+    assert o.wcc is True and o.trim2 is True and o.heavy_degree == 1024
