@@ -72,7 +72,7 @@ class scc_stats(C.Structure):
 class scc_server_cfg(C.Structure):
     _fields_ = [
         ("device", C.c_int32), ("batching", C.c_int32), ("max_batch_graphs", C.c_uint32),
-        ("max_batch_vertices", C.c_uint32), ("max_batch_edges", C.c_uint32), ("pad", C.c_uint32),
+        ("max_batch_vertices", C.c_uint32), ("max_batch_edges", C.c_uint32), ("solo_vertices", C.c_uint32),
         ("mem_budget", C.c_uint64), ("opts", scc_opts),
     ]
 

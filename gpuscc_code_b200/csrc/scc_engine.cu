@@ -24,7 +24,7 @@
 
 namespace sccb {
 
-enum : uint32_t { C_CHG = 0, C_DEG = 1, C_Q = 2, C_Q2 = 3, C_CNT = 4, C_CNT2 = 5 };
+enum : uint32_t { C_CHG = 0, C_DEG = 1, C_Q = 2, C_Q2 = 3, C_CNT = 4, C_CNT2 = 5, C_REM = 6 };
 enum : uint32_t { ARM_Q = 0, ARM_T = 1, ARM_D = 2, ARM_L = 3, ARM_B = 6 };
 
 constexpr int kSlotCache = 128;  // per-CTA cache of partition-election slots
@@ -145,35 +145,39 @@ struct Eng {
   // current one, so their latency overlaps the current vertex's dependent
   // chain.  load() may only read data that f() of the same iteration does
   // not change for other lanes' vertices (bitmap words, offsets, ranges).
+  // The same over an explicit list lst[0, cnt): two-deep, the entry two
+  // iterations ahead and the per-vertex loads of the next entry are in
+  // flight while f runs on the current one.  Whole CTAs iterate together.
+  template <class L, class F>
+  __device__ void for_list_pf(const uint32_t *lst, uint32_t cnt, L &&load, F &&f) {
+    const uint32_t lim = (cnt + BS - 1u) / BS * BS;
+    const uint32_t stride = gstride();
+    uint32_t base = blockIdx.x * BS;
+    if (base >= lim) return;
+    const uint32_t i0 = base + threadIdx.x, i1 = i0 + stride;
+    bool val0 = i0 < cnt, val1 = i1 < cnt;
+    uint32_t v0 = val0 ? ldm(lst + i0) : 0u;
+    uint32_t v1 = val1 ? ldm(lst + i1) : 0u;
+    auto pre = load(v0, val0);
+    for (; base < lim; base += stride) {
+      const uint32_t i2 = base + 2u * stride + threadIdx.x;
+      const bool val2 = i2 < cnt;
+      const uint32_t v2 = val2 ? ldm(lst + i2) : 0u;
+      auto nxt = pre;
+      if (base + stride < lim) nxt = load(v1, val1);
+      f(v0, val0, pre);
+      pre = nxt;
+      v0 = v1;
+      val0 = val1;
+      v1 = v2;
+      val1 = val2;
+    }
+  }
+
   template <class L, class F>
   __device__ void for_vertices_pf(L &&load, F &&f) {
     if (list_mode) {
-      // two-deep: the list entry two iterations ahead and the per-vertex
-      // loads of the next entry are in flight while f runs on the current one
-      const uint32_t *lst = P.s.act[act_sel];
-      const uint32_t cnt = act_count;
-      const uint32_t lim = (cnt + BS - 1u) / BS * BS;
-      const uint32_t stride = gstride();
-      uint32_t base = blockIdx.x * BS;
-      if (base >= lim) return;
-      const uint32_t i0 = base + threadIdx.x, i1 = i0 + stride;
-      bool val0 = i0 < cnt, val1 = i1 < cnt;
-      uint32_t v0 = val0 ? ldm(lst + i0) : 0u;
-      uint32_t v1 = val1 ? ldm(lst + i1) : 0u;
-      auto pre = load(v0, val0);
-      for (; base < lim; base += stride) {
-        const uint32_t i2 = base + 2u * stride + threadIdx.x;
-        const bool val2 = i2 < cnt;
-        const uint32_t v2 = val2 ? ldm(lst + i2) : 0u;
-        auto nxt = pre;
-        if (base + stride < lim) nxt = load(v1, val1);
-        f(v0, val0, pre);
-        pre = nxt;
-        v0 = v1;
-        val0 = val1;
-        v1 = v2;
-        val1 = val2;
-      }
+      for_list_pf(P.s.act[act_sel], act_count, load, f);
       return;
     }
     const uint32_t lim = P.s.nwords * 32u;
@@ -203,19 +207,21 @@ struct Eng {
     uint32_t *dst;
     uint32_t *count;
     uint32_t cap;
-    uint32_t n;  // items staged by this warp (identical in all 32 lanes)
+    uint32_t n;     // items staged by this warp (identical in all 32 lanes)
+    uint32_t *buf;  // this warp's shared-memory segment (stage_buf)
   };
-  static constexpr uint32_t kStage = 256;
-  __device__ uint32_t *stage_buf() {
-    __shared__ uint32_t buf[BS / 32][kStage];
-    return buf[threadIdx.x >> 5];
+  static constexpr uint32_t kStage = BS >= 1024 ? 128 : 256;  // 2 segments per warp within 48 KB static
+  // which = 0 or 1: two independent segments per warp (a sweep may feed two lists)
+  __device__ uint32_t *stage_buf(uint32_t which = 0) {
+    __shared__ uint32_t buf[2][BS / 32][kStage];
+    return buf[which][threadIdx.x >> 5];
   }
   __device__ void stage_flush(Stage &q) {
     __syncwarp();
     uint32_t base = 0;
     if (lane_id() == 0 && q.n) base = atomicAdd(q.count, q.n);
     base = __shfl_sync(kFull, base, 0);
-    const uint32_t *buf = stage_buf();
+    const uint32_t *buf = q.buf;
     for (uint32_t i = lane_id(); i < q.n; i += 32) {
       const uint32_t pos = base + i;
       if (pos < q.cap) q.dst[pos] = buf[i];
@@ -228,7 +234,7 @@ struct Eng {
   __device__ void stage_put(Stage &q, bool pred, uint32_t v) {
     const uint32_t mask = __ballot_sync(kFull, pred);
     if (!mask) return;
-    if (pred) stage_buf()[q.n + __popc(mask & lanemask_lt())] = v;
+    if (pred) q.buf[q.n + __popc(mask & lanemask_lt())] = v;
     q.n += __popc(mask);
     if (q.n > kStage - 32) stage_flush(q);
   }
@@ -288,7 +294,7 @@ struct Eng {
     unsigned long long t0 = globaltimer_ns();
     uint32_t ntrim = 0;
     unsigned long long best = ~0ull;
-    Stage tq{s.qa, cur() + C_Q, s.qcap, 0};
+    Stage tq{s.qa, cur() + C_Q, s.qcap, 0, stage_buf()};
     struct Pre {
       uint32_t ew, a0, a1, b0, b1;
     };
@@ -731,6 +737,10 @@ struct Eng {
     uint32_t depth = 0, sel = 0;
     unsigned long long explored = 0, mf = 0;
     bool pull = false;
+    // unreached candidates of the last pull sweep (aux / pivkey are free during reach)
+    const uint32_t *rem_in = nullptr;
+    uint32_t rem_n = 0, rem_sel = 0;
+    bool rem_valid = false;
     while (nin > 0) {
       const unsigned long long ts = globaltimer_ns();
       if (allow_pull) {
@@ -752,7 +762,7 @@ struct Eng {
       if (pull) {
         slot = PR_PULL;
         if (is_lead()) atomicAdd(&c->pull_sweeps, 1u);
-        Stage pq{out, cnt, s.qcap, 0};
+        Stage pq{out, cnt, s.qcap, 0, stage_buf()};
         struct Pre {
           uint32_t vw, ew, pb, pe, ob, oe, rv;
         };
@@ -763,21 +773,45 @@ struct Eng {
           return Pre{ldm(vis + w),  ldm(s.elim + w),   ldg(poff + vv), ldg(poff + vv + 1),
                      ldg(off + vv), ldg(off + vv + 1), ranged ? ldm(s.range + vv) : 0u};
         };
-        for_vertices_pf(load, [&](uint32_t v, bool valid, const Pre &p) {
+        // Vertices a pull sweep examines but does not reach are kept in a
+        // list, and the next pull sweep of this reach examines only them.
+        uint32_t *rem_out = rem_sel ? s.pivkey : s.aux;
+        Stage rq{rem_out, cur() + C_REM, s.qcap, 0, stage_buf(1)};
+        auto body = [&](uint32_t v, bool valid, const Pre &p, bool aligned) {
           // whole warp = one bitmap word in full mode: skip words without a live unvisited vertex
-          if (!list_mode && (~p.vw & ~p.ew) == 0u) return;
+          if (aligned && (~p.vw & ~p.ew) == 0u) return;
           bool found = false;
-          if (valid && !(((p.vw | p.ew) >> (v & 31u)) & 1u)) {
+          const bool cand = valid && !(((p.vw | p.ew) >> (v & 31u)) & 1u);
+          if (cand) {
             found = any_visited(padj, p.pb, p.pe, vis, ranged, p.rv);
             if (found) degsum += p.oe - p.ob;
           }
-          warp_set_bits(vis, v, found, !list_mode);
+          warp_set_bits(vis, v, found, aligned);
           stage_put(pq, found, v);
-        });
+          stage_put(rq, cand && !found, v);
+        };
+        if (rem_valid) {
+          for_list_pf(rem_in, rem_n, load, [&](uint32_t v, bool valid, const Pre &p) { body(v, valid, p, false); });
+        } else {
+          for_vertices_pf(load, [&](uint32_t v, bool valid, const Pre &p) { body(v, valid, p, !list_mode); });
+        }
         stage_flush(pq);
+        stage_flush(rq);
         add_count(cur() + C_DEG, degsum);
         if (!bar(703)) return depth;
+        rem_in = rem_out;
+        rem_n = rdprv(C_REM);
+        rem_valid = true;
+        rem_sel ^= 1u;
       } else if (balanced) {
+        rem_valid = false;
+        // with a small frontier, lists longer than a chunk go to the whole grid
+        // (one warp would otherwise walk thousands of edges while the rest wait)
+        // (at most nwarps lists qualify, so the heavy-list counter sees few atomics);
+        // mf (the frontier's edges) is known only where pulls are allowed
+        const unsigned long long per_warp = mf / nwarps();
+        uint32_t split = heavy;
+        if (allow_pull && per_warp < heavy) split = per_warp < 256ull ? 256u : (uint32_t)per_warp;
         for_items(nin, [&](uint32_t i, bool valid) {
           uint32_t v = 0, b = 0, d = 0, rv = 0;
           if (valid) {
@@ -785,7 +819,7 @@ struct Eng {
             b = ldg(off + v);
             d = ldg(off + v + 1) - b;
             rv = ranged ? ldm(s.range + v) : 0u;
-            if (d > heavy) {
+            if (d > split) {
               heavy_push(v, b, d, rv);
               d = 0;
             }
@@ -982,7 +1016,7 @@ struct Eng {
   // ============================================= active-list compaction
   __device__ void compact() {
     const EngState &s = P.s;
-    Stage aq{s.act[act_sel ^ 1u], cur() + C_Q, s.qcap, 0};
+    Stage aq{s.act[act_sel ^ 1u], cur() + C_Q, s.qcap, 0, stage_buf()};
     for_vertices([&](uint32_t v, bool valid) {
       const uint32_t ew = ldm(s.elim + (v >> 5));
       if (!list_mode && ~ew == 0u) return;  // whole word eliminated

@@ -381,6 +381,8 @@ void scc_server::solve_loop() {
       uint64_t nv = 0, ne = 0;
       for (Request *r : ready) {
         if (batch.size() >= max_g) break;
+        if (!batch.empty() && batch[0]->g.n > cfg.solo_vertices) break;  // a large graph goes alone
+        if (!batch.empty() && r->g.n > cfg.solo_vertices) continue;
         if (!batch.empty() && std::memcmp(r->choice, batch[0]->choice, sizeof(r->choice)) != 0) continue;
         if (!batch.empty() && (nv + r->g.n > cfg.max_batch_vertices || ne + r->g.m > cfg.max_batch_edges)) continue;
         batch.push_back(r);
@@ -410,6 +412,7 @@ void scc_server_cfg_default(scc_server_cfg *cfg) {
   cfg->max_batch_graphs = 256;
   cfg->max_batch_vertices = 1u << 24;
   cfg->max_batch_edges = 1u << 27;
+  cfg->solo_vertices = 1u << 18;
   scc_opts_default(&cfg->opts);
   cfg->opts.alg = SCC_ALG_HYBRID;
   cfg->opts.wcc = 1;
@@ -425,6 +428,7 @@ int scc_server_start(const scc_server_cfg *cfg, scc_server **out) {
   if (!s->cfg.max_batch_graphs) s->cfg.max_batch_graphs = 256;
   if (!s->cfg.max_batch_vertices) s->cfg.max_batch_vertices = 1u << 24;
   if (!s->cfg.max_batch_edges) s->cfg.max_batch_edges = 1u << 27;
+  if (!s->cfg.solo_vertices) s->cfg.solo_vertices = 1u << 18;
   if (s->cfg.max_batch_vertices >= (1u << 30)) return sccb::set_error(SCC_ERR_INVALID, "max_batch_vertices >= 2^30");
   SCK(cudaSetDevice(cfg->device), "cudaSetDevice");
   int rc = scc_ctx_create(cfg->device, &cfg->opts, &s->ctx);

@@ -26,7 +26,7 @@ class Server:
 
     def __init__(self, device: int = 0, options: Options | None = None, batching: bool = True,
                  max_batch_graphs: int = 256, max_batch_vertices: int = 1 << 24, max_batch_edges: int = 1 << 27,
-                 mem_budget: int = 0, model=None):
+                 solo_vertices: int = 1 << 18, mem_budget: int = 0, model=None):
         cfg = scc_server_cfg()
         lib.scc_server_cfg_default(C.byref(cfg))
         cfg.device = device
@@ -34,6 +34,7 @@ class Server:
         cfg.max_batch_graphs = max_batch_graphs
         cfg.max_batch_vertices = max_batch_vertices
         cfg.max_batch_edges = max_batch_edges
+        cfg.solo_vertices = solo_vertices
         cfg.mem_budget = mem_budget
         if options is not None:
             cfg.opts = options.to_c()
@@ -61,8 +62,11 @@ class Server:
         check(lib.scc_server_set_model(self._h, params.ctypes.data_as(fp), mean.ctypes.data_as(fp),
                                        scale.ctypes.data_as(fp)))
 
-    def submit(self, g: HostCSR) -> int:
-        labels = np.zeros(g.n + 1, np.uint32)
+    def submit(self, g: HostCSR, out: np.ndarray | None = None) -> int:
+        """Queue g; its labels land in `out` (uint32, n+1; e.g. pinned) or a new array."""
+        labels = np.zeros(g.n + 1, np.uint32) if out is None else out
+        if labels.dtype != np.uint32 or labels.size < g.n + 1 or not labels.flags.c_contiguous:
+            raise ValueError("out must be a contiguous uint32 array of n+1 entries")
         rid = C.c_uint64()
         check(lib.scc_server_submit(self._h, C.byref(g.raw), labels.ctypes.data_as(C.POINTER(C.c_uint32)),
                                     C.byref(rid)))
@@ -158,9 +162,10 @@ def poisson_arrivals(count: int, rate: float, seed: int = 5) -> np.ndarray:
     return np.cumsum(rng.exponential(1.0 / rate, size=count))
 
 
-def run_stream(server: Server, graphs, arrivals) -> dict:
-    """Submits graphs[i] at arrivals[i] seconds and waits for all of them.
-    Returns per-request latency, labels and the span of the run."""
+def run_stream(server: Server, graphs, arrivals, outs=None) -> dict:
+    """Submits graphs[i] at arrivals[i] seconds (labels into outs[i] when
+    given) and waits for all of them.  Returns per-request latency, labels
+    and the span of the run."""
     ids = [None] * len(graphs)
     results = [None] * len(graphs)
     t0 = time.perf_counter()
@@ -176,7 +181,7 @@ def run_stream(server: Server, graphs, arrivals) -> dict:
         delay = t0 + at - time.perf_counter()
         if delay > 0:
             time.sleep(delay)
-        ids[i] = server.submit(g)
+        ids[i] = server.submit(g, None if outs is None else outs[i])
         th = threading.Thread(target=waiter, args=(i,))
         th.start()
         threads.append(th)

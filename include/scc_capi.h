@@ -361,7 +361,9 @@ typedef struct scc_server_cfg {
   uint32_t max_batch_graphs;   /* 0 = 256 */
   uint32_t max_batch_vertices; /* capacity of the packed batch CSR (0 = 1<<24) */
   uint32_t max_batch_edges;    /* (0 = 1<<27) */
-  uint32_t pad;
+  uint32_t solo_vertices;      /* graphs with more vertices are solved alone: one such graph
+                                  already fills the device, and a batch runs as many rounds as
+                                  its slowest graph (0 = 1<<18) */
   uint64_t mem_budget;         /* device bytes for resident request graphs (0 = half the free memory) */
   scc_opts opts;               /* options of the plain method (and the base the network edits) */
 } scc_server_cfg;

@@ -86,3 +86,23 @@ def test_features_of_a_small_graph_by_hand():
     ln = np.log2(7.0)
     assert f[13] == pytest.approx(np.log2(3) / ln) and f[14] == pytest.approx(np.log2(3) / ln)
     assert f[15] == 0.0
+
+
+def test_shipped_network_on_recorded_traces():
+    """The shipped parameters (trained on the device from the recorded traces
+    of plain-method runs on a B200) read back through the CPU oracle pick
+    choices that cost less than the plain hybrid on those traces."""
+    from pathlib import Path
+    root = Path(__file__).resolve().parents[1]
+    net = np.load(root / "gpuscc_code_b200" / "strategy_net.npz")
+    tr = np.load(root / "tests" / "golden" / "strategy_traces.npz")
+    X, T = tr["X"], tr["T"]
+    assert net["params"].size == mo.N_PARAMS and X.shape[1] == 16 and T.shape[1] == 16
+    picks = mo.predict(net["params"].astype(np.float64), X, net["mean"], net["scale"])
+    import itertools
+    choices = list(itertools.product(range(2), range(2), range(4)))
+    idx = np.array([choices.index(tuple(int(v) for v in p)) for p in picks])
+    learned = T[np.arange(len(T)), idx].sum()
+    plain = T[:, 0].sum()
+    assert learned < plain
+    assert learned <= 1.1 * T.min(axis=1).sum()
