@@ -24,7 +24,15 @@
 
 namespace sccb {
 
-enum : uint32_t { C_CHG = 0, C_DEG = 1, C_Q = 2, C_Q2 = 3, C_CNT = 4, C_CNT2 = 5, C_REM = 6 };
+enum : uint32_t {
+  C_CHG = 0, C_DEG = 1, C_Q = 2, C_Q2 = 3, C_CNT = 4, C_CNT2 = 5, C_REM = 6,
+  // results of a run of CTA-local levels (reach_wl)
+  C_LN = 7, C_LSEL = 8, C_LD = 9, C_LMF = 10, C_LEX = 11, C_LREF = 12
+};
+// CTA-local reach levels: frontiers of at most kLocalMax vertices and
+// kLocalEdges edges are expanded by CTA 0 alone with CTA barriers, at most
+// kLocalLevels levels per grid barrier
+constexpr uint32_t kLocalMax = 2048, kLocalEdges = 4096, kLocalLevels = 4096;
 enum : uint32_t { ARM_Q = 0, ARM_T = 1, ARM_D = 2, ARM_L = 3, ARM_B = 6 };
 
 constexpr int kSlotCache = 128;  // per-CTA cache of partition-election slots
@@ -288,12 +296,114 @@ struct Eng {
   // previous one (deduplicated through the `queued` bitmap).
   // pick: also elect the first pivot among the survivors of the sweep (only
   // valid when no further trim iteration follows, i.e. max_it == 1).
+  // The first trim sweep when nothing is eliminated yet and every list is
+  // sorted-unique: only degrees decide (a list of one entry counts unless it
+  // is a self-loop).  Each thread takes four consecutive ids with one 16-byte
+  // load of each offset array (the fifth offset comes from the next lane), so
+  // a warp covers four bitmap words per iteration; eliminated/trimmed words
+  // are assembled in registers.  Returns this thread's count of trimmed ids.
+  __device__ uint32_t trim_snap_sweep(bool pick, unsigned long long &best) {
+    const EngState &s = P.s;
+    const EngGraph &g = P.g;
+    const uint32_t n = g.n;
+    const uint32_t lim = s.nwords * 32u;  // multiple of 1024
+    const uint32_t lane = lane_id();
+    const bool vec = ((reinterpret_cast<uintptr_t>(g.off) | reinterpret_cast<uintptr_t>(g.offT)) & 15u) == 0;
+    const uint32_t step = gstride() * 4u;
+    struct Quad {
+      uint32_t o[4], t[4];
+    };
+    auto load = [&](uint32_t v0) {
+      Quad q;
+      if (vec && v0 + 4u <= n + 2u) {  // off / offT hold n+2 entries
+        const uint4 a = __ldg(reinterpret_cast<const uint4 *>(g.off + v0));
+        const uint4 b = __ldg(reinterpret_cast<const uint4 *>(g.offT + v0));
+        q.o[0] = a.x, q.o[1] = a.y, q.o[2] = a.z, q.o[3] = a.w;
+        q.t[0] = b.x, q.t[1] = b.y, q.t[2] = b.z, q.t[3] = b.w;
+      } else {
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          const bool in = v0 + i <= n + 1u;
+          q.o[i] = in ? ldg(g.off + v0 + i) : 0u;
+          q.t[i] = in ? ldg(g.offT + v0 + i) : 0u;
+        }
+      }
+      return q;
+    };
+    uint32_t ntrim = 0;
+    uint32_t base = blockIdx.x * BS * 4u;
+    const uint32_t wofs = (threadIdx.x >> 5) * 128u + lane * 4u;
+    if (base >= lim) return 0;
+    Quad cur_q = load(base + wofs);
+    for (; base < lim; base += step) {
+      const uint32_t v0 = base + wofs;
+      // next iteration's offsets are in flight while this one is decided
+      Quad nxt = cur_q;
+      if (base + step < lim) nxt = load(base + step + wofs);
+      const Quad &q = cur_q;
+      uint32_t o4 = __shfl_down_sync(kFull, q.o[0], 1), t4 = __shfl_down_sync(kFull, q.t[0], 1);
+      if (lane == 31) {
+        const bool in = v0 + 4u <= n + 1u;
+        o4 = in ? ldg(g.off + v0 + 4u) : 0u;
+        t4 = in ? ldg(g.offT + v0 + 4u) : 0u;
+      }
+      // degrees first; the single-entry lists' heads (self-loop test) are
+      // loaded together, and only where the other direction does not decide
+      uint32_t dout[4], din[4], x[4], y[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        dout[i] = (i < 3 ? q.o[i + 1] : o4) - q.o[i];
+        din[i] = (i < 3 ? q.t[i + 1] : t4) - q.t[i];
+        const bool valid = v0 + i >= 1u && v0 + i <= n;
+        const bool open = valid && dout[i] != 0 && din[i] != 0;
+        x[i] = (open && dout[i] == 1) ? ldg(g.adj + q.o[i]) : 0u;
+        y[i] = (open && din[i] == 1) ? ldg(g.adjT + q.t[i]) : 0u;
+      }
+      uint32_t bits = 0;
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const uint32_t v = v0 + i;
+        if (v < 1u || v > n) continue;
+        const bool tr = dout[i] == 0 || din[i] == 0 || (dout[i] == 1 && x[i] == v) || (din[i] == 1 && y[i] == v);
+        if (tr) {
+          s.label[v] = v;
+          bits |= 1u << i;
+          ++ntrim;
+        } else if (pick) {
+          const unsigned long long key = ((unsigned long long)prio(v) << 32) | v;
+          best = key < best ? key : best;
+        }
+      }
+      // lanes 8j .. 8j+7 hold the 32 ids of word j of this warp's four
+      const uint32_t grp = 0xffu << (lane & ~7u);
+      const uint32_t word = __reduce_or_sync(grp, bits << (4u * (lane & 7u)));
+      if ((lane & 7u) == 0 && word) {
+        const uint32_t w = (v0 >> 5);
+        atomicOr(s.elim + w, word);
+        atomicOr(s.tflag + w, word);
+      }
+      cur_q = nxt;
+    }
+    return ntrim;
+  }
+
   __device__ uint32_t trim(bool ranged, bool snap, uint32_t max_it, bool pick = false) {
     const EngState &s = P.s;
     const EngGraph &g = P.g;
     unsigned long long t0 = globaltimer_ns();
     uint32_t ntrim = 0;
     unsigned long long best = ~0ull;
+    if (snap && !ranged && max_it == 1 && !list_mode) {
+      ntrim = trim_snap_sweep(pick, best);
+      add_count(&c->n_trimmed, ntrim);
+      if (pick) {
+        best = block_min_u64(best);
+        if (threadIdx.x == 0 && best != ~0ull) atomicMin(&c->best, best);
+      }
+      if (!bar(100)) return 1;
+      prof(PR_TRIM_SWEEP, t0, 0);
+      return 1;
+    }
     Stage tq{s.qa, cur() + C_Q, s.qcap, 0, stage_buf()};
     struct Pre {
       uint32_t ew, a0, a1, b0, b1;
@@ -592,9 +702,26 @@ struct Eng {
     // 16-byte loads only when the list base is 16-byte aligned (caller-bound
     // graphs may not be); otherwise the scalar tail loop below does it all
     const bool vec = (reinterpret_cast<uintptr_t>(adj) & 15u) == 0;
-    while (vec && i < e && (i & 3u)) {
-      if (hit(ldg(adj + i))) return true;
-      ++i;
+    if (vec && i < e && (i & 3u)) {
+      // the aligned 16 bytes holding the list head (entries of the previous
+      // list masked off) instead of up to three dependent scalar probes
+      const uint32_t a = i & ~3u;
+      if ((unsigned long long)a + 4ull <= P.g.m) {
+        const uint4 q = __ldg(reinterpret_cast<const uint4 *>(adj + a));
+        const uint32_t u[4] = {q.x, q.y, q.z, q.w};
+        uint32_t w[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) w[j] = (a + j >= i && a + j < e) ? ldm(vis + (u[j] >> 5)) : 0u;
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+          if (((w[j] >> (u[j] & 31u)) & 1u) && (!ranged || ldm(rng + u[j]) == rv)) return true;
+        i = a + 4u;
+      } else {
+        while (i < e && (i & 3u)) {
+          if (hit(ldg(adj + i))) return true;
+          ++i;
+        }
+      }
     }
     if (!ranged) {  // eight probes in flight per step
       for (; vec && i + 8 <= e; i += 8) {
@@ -633,26 +760,43 @@ struct Eng {
   // not yet expanded vertex, one thread per vertex.
   __device__ uint32_t reach_q(const uint32_t *__restrict__ off, const uint32_t *__restrict__ adj, uint32_t *vis,
                               uint32_t *exp, bool ranged) {
+    const uint32_t heavy = P.o.heavy_degree;
     uint32_t depth = 0;
     for (;;) {
       const unsigned long long ts = globaltimer_ns();
       uint32_t chg = 0;
+      auto visit = [&](uint32_t, uint32_t u, uint32_t rsrc) { chg += try_visit(vis, u, ranged, rsrc); };
       for_vertices([&](uint32_t v, bool valid) {
         // No warp-level "skip this word" shortcut here: visit bits change
-        // under other warps during the sweep, and lanes left diverged by the
-        // previous iteration's expansions read the word at different times,
-        // so such a test is not warp-uniform and would strand the lanes that
-        // enter the ballot below.  (The shortcuts in trim, pull, update and
-        // compaction test words only their own warp changes.)
+        // under other warps during the sweep, so such a test would not be
+        // warp-uniform.  The lists of this sweep's frontier vertices are
+        // walked by the whole warp (warp_gather); a list longer than
+        // heavy_degree goes to the grid (one hub's list would otherwise keep
+        // a single thread busy for the whole sweep).
         const bool fr = valid && live(v) && bit_test(vis, v) && !bit_test(exp, v);
         warp_set_bits(exp, v, fr, !list_mode);
-        if (!fr) return;
-        const uint32_t rv = ranged ? ldm(P.s.range + v) : 0u;
-        const uint32_t b = ldg(off + v), e = ldg(off + v + 1);
-        for (uint32_t i = b; i < e; ++i) chg += try_visit(vis, ldg(adj + i), ranged, rv);
+        uint32_t b = 0, d = 0, rv = 0;
+        if (fr) {
+          rv = ranged ? ldm(P.s.range + v) : 0u;
+          b = ldg(off + v);
+          d = ldg(off + v + 1) - b;
+          if (d > heavy) {
+            heavy_push(v, b, d, rv);
+            d = 0;
+          }
+        }
+        warp_gather(v, b, d, rv, adj, visit);
       });
       add_count(cur() + C_CHG, chg);
       if (!bar(500)) return depth;
+      const unsigned long long h = ldm64(prv64());
+      if ((uint32_t)(h >> 32) != 0) {
+        if (is_lead()) atomicAdd(cur() + C_CHG, rdprv(C_CHG));
+        chg = 0;
+        heavy_expand(adj, h, visit);
+        add_count(cur() + C_CHG, chg);
+        if (!bar(501)) return depth;
+      }
       prof(PR_Q, ts, rdprv(C_CHG));
       ++depth;
       if (rdprv(C_CHG) == 0) break;
@@ -724,6 +868,83 @@ struct Eng {
   // edges / alpha, a level becomes a pull sweep -- every live unvisited
   // vertex scans its reverse list for a visited partition-mate -- until fewer
   // than live / beta vertices are reached per sweep.
+  // Push levels run by CTA 0 alone while the frontier stays small (high-
+  // diameter graphs spend hundreds of levels on a few dozen vertices each,
+  // where a grid barrier per level costs more than the level).  Same visit
+  // rule as the grid levels; the next frontier goes to the other queue
+  // through a shared-memory counter.  Results land in the counters C_L*.
+  // The frontier's edges are checked first: too many and nothing is done
+  // (C_LREF = 1), the grid expands that level instead.
+  __device__ void local_levels(const uint32_t *__restrict__ off, const uint32_t *__restrict__ adj, uint32_t *vis,
+                               bool ranged, const uint32_t *in, uint32_t nin, uint32_t sel, uint32_t max_levels) {
+    const EngState &s = P.s;
+    __shared__ uint32_t s_cnt, s_deg;
+    uint32_t d = 0;
+    for (uint32_t i = threadIdx.x; i < nin; i += BS) {
+      const uint32_t v = ldm(in + i);
+      d += ldg(off + v + 1) - ldg(off + v);
+    }
+    d = block_sum(d);
+    if (threadIdx.x == 0) s_deg = d;
+    __syncthreads();
+    uint32_t lmf = s_deg;
+    __syncthreads();
+    if (lmf > kLocalEdges) {
+      if (threadIdx.x == 0) cur()[C_LREF] = 1u;
+      return;
+    }
+    uint32_t lnin = nin, ld = 0, lsel = sel, lex = 0;
+    const uint32_t *lin = in;
+    while (lnin > 0 && ld < max_levels) {
+      uint32_t *lout = lsel ? s.qb : s.qa;
+      if (threadIdx.x == 0) {
+        s_cnt = 0;
+        s_deg = 0;
+      }
+      __syncthreads();
+      uint32_t degsum = 0;
+      auto visit = [&](uint32_t, uint32_t u, uint32_t rsrc) {
+        if (try_visit(vis, u, ranged, rsrc)) {
+          const uint32_t pos = atomicAdd(&s_cnt, 1u);
+          if (pos < s.qcap) lout[pos] = u;
+          else fail(kErrQueueOverflow);
+          degsum += ldg(off + u + 1) - ldg(off + u);
+        }
+      };
+      const uint32_t lim = (lnin + BS - 1u) / BS * BS;
+      for (uint32_t base = 0; base < lim; base += BS) {
+        const uint32_t i = base + threadIdx.x;
+        uint32_t v = 0, b = 0, dd = 0, rv = 0;
+        if (i < lnin) {
+          v = ldm(lin + i);
+          b = ldg(off + v);
+          dd = ldg(off + v + 1) - b;
+          rv = ranged ? ldm(s.range + v) : 0u;
+        }
+        warp_gather(v, b, dd, rv, adj, visit);
+      }
+      degsum = __reduce_add_sync(kFull, degsum);
+      if (lane_id() == 0 && degsum) atomicAdd(&s_deg, degsum);
+      __syncthreads();
+      lnin = s_cnt;
+      lmf = s_deg;
+      lex += lmf;
+      ++ld;
+      lin = lout;
+      lsel ^= 1u;
+      __syncthreads();
+      if (lnin > kLocalMax || lmf > kLocalEdges) break;
+    }
+    if (threadIdx.x == 0) {
+      uint32_t *o = cur();
+      o[C_LN] = lnin;
+      o[C_LSEL] = lsel;
+      o[C_LD] = ld;
+      o[C_LMF] = lmf;
+      o[C_LEX] = lex;
+    }
+  }
+
   __device__ uint32_t reach_wl(const uint32_t *__restrict__ off, const uint32_t *__restrict__ adj,
                                const uint32_t *__restrict__ poff, const uint32_t *__restrict__ padj, uint32_t *vis,
                                bool ranged, bool balanced, bool allow_pull) {
@@ -743,6 +964,29 @@ struct Eng {
     bool rem_valid = false;
     while (nin > 0) {
       const unsigned long long ts = globaltimer_ns();
+      // a small frontier goes to CTA 0; if it refuses (too many edges), the
+      // grid expands this level as usual and the next level tries again
+      if (!pull && nin <= kLocalMax) {
+        const uint32_t room = P.o.max_iters > depth ? P.o.max_iters - depth : 0u;
+        if (blockIdx.x == 0) local_levels(off, adj, vis, ranged, in, nin, sel, room < kLocalLevels ? room : kLocalLevels);
+        if (!bar(704)) return depth;
+        if (!rdprv(C_LREF) && rdprv(C_LD) > 0) {
+          const uint32_t ld = rdprv(C_LD);
+          depth += ld;
+          nin = rdprv(C_LN);
+          mf = rdprv(C_LMF);
+          explored += rdprv(C_LEX);
+          sel = rdprv(C_LSEL);
+          in = sel ? s.qa : s.qb;  // the queue the last local level filled
+          rem_valid = false;
+          prof(PR_WL, ts, ld, nin);
+          if (depth >= P.o.max_iters) {
+            fail(kErrIterCap);
+            break;
+          }
+          continue;
+        }
+      }
       if (allow_pull) {
         const unsigned long long unexplored = mtot > explored ? mtot - explored : 0ull;
         if (!pull && depth > 0 && (long long)mf * alpha > (long long)unexplored) pull = true;
@@ -949,9 +1193,16 @@ struct Eng {
   // inside the partition (min-label propagation plus pointer jumping, to a
   // fixpoint); each colour becomes a partition whose pivot is the colour's
   // root.  The colour is constant on an SCC, so no SCC is split.
+  // wcc.cu:7-226: colour = smallest id reachable inside the partition along
+  // out-edges, with one pointer jump per sweep; SCC members share a colour.
+  // Labels only decrease and always name a vertex reachable from the one
+  // they label, so updates may land in any order (atomicMin) and the fixpoint
+  // is the same.  Lists are walked warp-wide, lists longer than heavy_degree
+  // by the whole grid.
   __device__ uint32_t wcc() {
     const EngState &s = P.s;
     const EngGraph &g = P.g;
+    const uint32_t heavy = P.o.heavy_degree;
     uint32_t *lab = s.aux;
     for_vertices([&](uint32_t v, bool valid) {
       if (valid && live(v)) lab[v] = v;
@@ -960,27 +1211,40 @@ struct Eng {
     uint32_t it = 0;
     for (;;) {
       uint32_t chg = 0;
+      // called from divergent code (warp_gather tails, heavy chunks): no warp collectives
+      auto relax = [&](uint32_t src, uint32_t u, uint32_t rsrc) {
+        if (!live(u) || ldm(s.range + u) != rsrc) return;
+        const uint32_t x = ldm(lab + u);
+        if (x < ldm(lab + src)) chg += atomicMin(lab + src, x) > x;
+      };
       for_vertices([&](uint32_t v, bool valid) {
-        if (!valid || !live(v)) return;
-        const uint32_t old = ldm(lab + v);
-        uint32_t m = old;
-        const uint32_t rv = ldm(s.range + v);
-        const uint32_t b = ldg(g.off + v), e = ldg(g.off + v + 1);
-        for (uint32_t i = b; i < e; ++i) {
-          const uint32_t u = ldg(g.adj + i);
-          if (!live(u) || ldm(s.range + u) != rv) continue;
-          const uint32_t x = ldm(lab + u);
-          m = x < m ? x : m;
+        uint32_t b = 0, d = 0, rv = 0;
+        const bool lv = valid && live(v);
+        if (lv) {
+          rv = ldm(s.range + v);
+          b = ldg(g.off + v);
+          d = ldg(g.off + v + 1) - b;
+          if (d > heavy) {
+            heavy_push(v, b, d, rv);
+            d = 0;
+          }
         }
-        const uint32_t j = ldm(lab + m);
-        m = j < m ? j : m;
-        if (m < old) {
-          lab[v] = m;
-          ++chg;
+        warp_gather(v, b, d, rv, g.adj, relax);
+        if (lv) {  // pointer jump
+          const uint32_t m = ldm(lab + v), j = ldm(lab + m);
+          if (j < m) chg += atomicMin(lab + v, j) > j;
         }
       });
       add_count(cur() + C_CHG, chg);
       if (!bar(901)) return it;
+      const unsigned long long h = ldm64(prv64());
+      if ((uint32_t)(h >> 32) != 0) {
+        if (is_lead()) atomicAdd(cur() + C_CHG, rdprv(C_CHG));
+        chg = 0;
+        heavy_expand(g.adj, h, relax);
+        add_count(cur() + C_CHG, chg);
+        if (!bar(904)) return it;
+      }
       ++it;
       if (rdprv(C_CHG) == 0) break;
       if (it >= P.o.max_iters) {
@@ -1016,13 +1280,37 @@ struct Eng {
   // ============================================= active-list compaction
   __device__ void compact() {
     const EngState &s = P.s;
-    Stage aq{s.act[act_sel ^ 1u], cur() + C_Q, s.qcap, 0, stage_buf()};
-    for_vertices([&](uint32_t v, bool valid) {
-      const uint32_t ew = ldm(s.elim + (v >> 5));
-      if (!list_mode && ~ew == 0u) return;  // whole word eliminated
-      stage_put(aq, valid && !((ew >> (v & 31u)) & 1u), v);
-    });
-    stage_flush(aq);
+    uint32_t *dst = s.act[act_sel ^ 1u];
+    if (!list_mode) {
+      // one bitmap word per lane (ids 0 and > n are marked eliminated at
+      // init): a warp covers 1024 ids per step, scans its live counts and
+      // appends them with one atomicAdd, each lane its word's ids in order
+      const uint32_t lane = lane_id();
+      for (uint32_t w0 = gwarp() * 32u; w0 < s.nwords; w0 += nwarps() * 32u) {
+        const uint32_t w = w0 + lane;
+        uint32_t live = w < s.nwords ? ~ldm(s.elim + w) : 0u;
+        const uint32_t cnt = __popc(live);
+        const uint32_t incl = warp_incl_scan(cnt);
+        uint32_t base = 0;
+        if (lane == 31 && incl) base = atomicAdd(cur() + C_Q, incl);
+        base = __shfl_sync(kFull, base, 31);
+        uint32_t pos = base + incl - cnt;
+        while (live) {
+          const uint32_t b = __ffs(live) - 1u;
+          if (pos < s.qcap) dst[pos] = w * 32u + b;
+          else fail(kErrQueueOverflow);
+          ++pos;
+          live &= live - 1u;
+        }
+      }
+    } else {
+      Stage aq{dst, cur() + C_Q, s.qcap, 0, stage_buf()};
+      for_vertices([&](uint32_t v, bool valid) {
+        const uint32_t ew = ldm(s.elim + (v >> 5));
+        stage_put(aq, valid && !((ew >> (v & 31u)) & 1u), v);
+      });
+      stage_flush(aq);
+    }
     if (!bar(1000)) return;
     if (is_lead()) {
       c->act_count = rdprv(C_Q);
