@@ -182,6 +182,45 @@ struct Eng {
     }
   }
 
+  // Three stages over a list: the entry three iterations ahead, load1 (per-
+  // vertex words and offsets) two ahead, load2 (reads that need load1's
+  // results, e.g. the head of an adjacency list) one ahead; then f(v, valid,
+  // pre1, pre2) on the current entry.
+  template <class L1, class L2, class F>
+  __device__ void for_list_pf3(const uint32_t *lst, uint32_t cnt, L1 &&load1, L2 &&load2, F &&f) {
+    const uint32_t lim = (cnt + BS - 1u) / BS * BS;
+    const uint32_t stride = gstride();
+    uint32_t base = blockIdx.x * BS;
+    if (base >= lim) return;
+    const uint32_t i0 = base + threadIdx.x;
+    bool val0 = i0 < cnt, val1 = i0 + stride < cnt, val2 = i0 + 2u * stride < cnt;
+    uint32_t v0 = val0 ? ldm(lst + i0) : 0u;
+    uint32_t v1 = val1 ? ldm(lst + i0 + stride) : 0u;
+    uint32_t v2 = val2 ? ldm(lst + i0 + 2u * stride) : 0u;
+    auto p0 = load1(v0, val0);
+    auto p1 = load1(v1, val1);
+    auto h0 = load2(v0, val0, p0);
+    for (; base < lim; base += stride) {
+      const uint32_t i3 = base + 3u * stride + threadIdx.x;
+      const bool val3 = i3 < cnt;
+      const uint32_t v3 = val3 ? ldm(lst + i3) : 0u;
+      auto p2 = p1;
+      if (base + 2u * stride < lim) p2 = load1(v2, val2);
+      auto h1 = h0;
+      if (base + stride < lim) h1 = load2(v1, val1, p1);
+      f(v0, val0, p0, h0);
+      p0 = p1;
+      p1 = p2;
+      h0 = h1;
+      v0 = v1;
+      val0 = val1;
+      v1 = v2;
+      val1 = val2;
+      v2 = v3;
+      val2 = val3;
+    }
+  }
+
   template <class L, class F>
   __device__ void for_vertices_pf(L &&load, F &&f) {
     if (list_mode) {
@@ -692,8 +731,10 @@ struct Eng {
   // four entries at a time (one 16-byte load once aligned) and the four
   // bitmap words are requested together, so a thread keeps several
   // independent L2 requests in flight instead of one dependent chain.
+  // head: the aligned 16 bytes holding adj[b] when the caller loaded them
+  // ahead (pull_head below), else nullptr.
   __device__ bool any_visited(const uint32_t *__restrict__ adj, uint32_t b, uint32_t e, const uint32_t *vis,
-                              bool ranged, uint32_t rv) {
+                              bool ranged, uint32_t rv, const uint4 *head = nullptr) {
     const uint32_t *rng = P.s.range;
     auto hit = [&](uint32_t u) {
       return ((ldm(vis + (u >> 5)) >> (u & 31u)) & 1u) && (!ranged || ldm(rng + u) == rv);
@@ -702,12 +743,12 @@ struct Eng {
     // 16-byte loads only when the list base is 16-byte aligned (caller-bound
     // graphs may not be); otherwise the scalar tail loop below does it all
     const bool vec = (reinterpret_cast<uintptr_t>(adj) & 15u) == 0;
-    if (vec && i < e && (i & 3u)) {
+    if (vec && i < e && ((i & 3u) || head)) {
       // the aligned 16 bytes holding the list head (entries of the previous
       // list masked off) instead of up to three dependent scalar probes
       const uint32_t a = i & ~3u;
       if ((unsigned long long)a + 4ull <= P.g.m) {
-        const uint4 q = __ldg(reinterpret_cast<const uint4 *>(adj + a));
+        const uint4 q = head ? *head : __ldg(reinterpret_cast<const uint4 *>(adj + a));
         const uint32_t u[4] = {q.x, q.y, q.z, q.w};
         uint32_t w[4];
 #pragma unroll
@@ -1008,36 +1049,56 @@ struct Eng {
         if (is_lead()) atomicAdd(&c->pull_sweeps, 1u);
         Stage pq{out, cnt, s.qcap, 0, stage_buf()};
         struct Pre {
-          uint32_t vw, ew, pb, pe, ob, oe, rv;
+          uint32_t vw, ew, pb, pe, rv;
         };
         // Only v's own lane sets v's visit bit during a pull sweep, so the
-        // prefetched word is current for the bit this lane tests.
+        // prefetched word is current for the bit this lane tests.  The
+        // frontier's edge count (for the direction heuristics) is taken from
+        // the reverse lists already loaded: in-degree stands in for
+        // out-degree, saving a random read of the other offsets per vertex.
         auto load = [&](uint32_t v, bool valid) {
           const uint32_t w = v >> 5, vv = valid ? v : 0u;
-          return Pre{ldm(vis + w),  ldm(s.elim + w),   ldg(poff + vv), ldg(poff + vv + 1),
-                     ldg(off + vv), ldg(off + vv + 1), ranged ? ldm(s.range + vv) : 0u};
+          return Pre{ldm(vis + w), ldm(s.elim + w), ldg(poff + vv), ldg(poff + vv + 1),
+                     ranged ? ldm(s.range + vv) : 0u};
         };
         // Vertices a pull sweep examines but does not reach are kept in a
         // list, and the next pull sweep of this reach examines only them.
         uint32_t *rem_out = rem_sel ? s.pivkey : s.aux;
         Stage rq{rem_out, cur() + C_REM, s.qcap, 0, stage_buf(1)};
-        auto body = [&](uint32_t v, bool valid, const Pre &p, bool aligned) {
+        auto body = [&](uint32_t v, bool valid, const Pre &p, bool aligned, const uint4 *head) {
           // whole warp = one bitmap word in full mode: skip words without a live unvisited vertex
           if (aligned && (~p.vw & ~p.ew) == 0u) return;
           bool found = false;
           const bool cand = valid && !(((p.vw | p.ew) >> (v & 31u)) & 1u);
           if (cand) {
-            found = any_visited(padj, p.pb, p.pe, vis, ranged, p.rv);
-            if (found) degsum += p.oe - p.ob;
+            found = any_visited(padj, p.pb, p.pe, vis, ranged, p.rv, head);
+            if (found) degsum += p.pe - p.pb;
           }
           warp_set_bits(vis, v, found, aligned);
           stage_put(pq, found, v);
           stage_put(rq, cand && !found, v);
         };
+        // list sweeps also load each candidate's list head one entry ahead
+        const bool head_ok = (reinterpret_cast<uintptr_t>(padj) & 15u) == 0;
+        auto head = [&](uint32_t v, bool valid, const Pre &p) {
+          uint4 q = make_uint4(0u, 0u, 0u, 0u);
+          const bool cand = valid && !(((p.vw | p.ew) >> (v & 31u)) & 1u);
+          const uint32_t a = p.pb & ~3u;
+          if (head_ok && cand && p.pe > p.pb && (unsigned long long)a + 4ull <= P.g.m)
+            q = __ldg(reinterpret_cast<const uint4 *>(padj + a));
+          return q;
+        };
+        auto list_body = [&](uint32_t v, bool valid, const Pre &p, const uint4 &q) {
+          const uint32_t a = p.pb & ~3u;
+          const bool have = head_ok && p.pe > p.pb && (unsigned long long)a + 4ull <= P.g.m;
+          body(v, valid, p, false, have ? &q : nullptr);
+        };
         if (rem_valid) {
-          for_list_pf(rem_in, rem_n, load, [&](uint32_t v, bool valid, const Pre &p) { body(v, valid, p, false); });
+          for_list_pf3(rem_in, rem_n, load, head, list_body);
+        } else if (list_mode) {
+          for_list_pf3(s.act[act_sel], act_count, load, head, list_body);
         } else {
-          for_vertices_pf(load, [&](uint32_t v, bool valid, const Pre &p) { body(v, valid, p, !list_mode); });
+          for_vertices_pf(load, [&](uint32_t v, bool valid, const Pre &p) { body(v, valid, p, true, nullptr); });
         }
         stage_flush(pq);
         stage_flush(rq);

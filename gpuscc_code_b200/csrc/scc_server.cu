@@ -135,6 +135,10 @@ struct scc_server {
   void solve_loop();
   int run_batch(std::vector<Request *> &batch);
   int choose(std::vector<Request *> &ready);
+  int pick(Request *r, cudaStream_t st, void *&scratch, size_t &bytes);
+  std::mutex mlp_mu;                  // the network's buffers are shared by both threads
+  void *admit_scratch = nullptr;      // feature scratch of the admission thread
+  size_t admit_bytes = 0;
   void finish(Request *r, int status);
 };
 
@@ -182,7 +186,18 @@ void scc_server::admit_loop() {
       if (e == cudaSuccess) e = cudaEventCreateWithFlags(&r->uploaded, cudaEventDisableTiming);
       if (e == cudaSuccess) e = cudaEventRecord(r->uploaded, copy_st);
     }
+    // with a network loaded, pick this request's options now, while earlier
+    // batches run (features run on the copy stream after the upload)
+    int prc = SCC_OK;
+    if (e == cudaSuccess && mlp) prc = pick(r, copy_st, admit_scratch, admit_bytes);
     lk.lock();
+    if (e == cudaSuccess && prc != SCC_OK) {
+      lk.unlock();
+      cudaStreamSynchronize(copy_st);
+      finish(r, prc);
+      lk.lock();
+      continue;
+    }
     if (e != cudaSuccess) {
       sccb::set_error(SCC_ERR_CUDA, "upload: %s", cudaGetErrorString(e));
       cudaStreamSynchronize(copy_st);  // nothing may still write into the allocation when it is freed
@@ -218,43 +233,46 @@ void scc_server::finish(Request *r, int status) {
 }
 
 // Features + network choice for the ready requests that have none yet.
-int scc_server::choose(std::vector<Request *> &ready) {
-  std::vector<Request *> todo;
-  for (Request *r : ready)
-    if (!r->have_choice) todo.push_back(r);
-  if (todo.empty()) return SCC_OK;
-  if (!mlp) {
-    for (Request *r : todo) r->have_choice = true;  // plain options: choice (0,0,0)
-    return SCC_OK;
+// Features of r's resident graph on stream st (ordered after its upload),
+// then the network's choice.  Scratch is the caller's (one per thread).
+int scc_server::pick(Request *r, cudaStream_t st, void *&scratch, size_t &bytes) {
+  const size_t need = sccb::features_scratch_bytes(r->g.n);
+  if (need > bytes) {
+    if (scratch) cudaFree(scratch);
+    scratch = nullptr;
+    bytes = 0;
+    SCK(cudaMalloc(&scratch, need), "alloc feature scratch");
+    bytes = need;
   }
-  std::vector<float> x(todo.size() * sccb::kFeatures);
-  for (size_t i = 0; i < todo.size(); ++i) {
-    Request *r = todo[i];
-    const size_t need = sccb::features_scratch_bytes(r->g.n);
-    if (need > feat_bytes) {
-      if (feat_scratch) cudaFree(feat_scratch);
-      feat_scratch = nullptr;
-      feat_bytes = 0;
-      SCK(cudaMalloc(&feat_scratch, need), "alloc feature scratch");
-      feat_bytes = need;
-    }
-    SCK(cudaStreamWaitEvent(solve_st, r->uploaded, 0), "wait upload");
-    sccb::EngGraph g{};
-    g.n = r->g.n;
-    g.m = r->g.m;
-    g.sorted_unique = r->g.sorted_unique ? 1u : 0u;
-    g.off = r->d_off();
-    g.adj = r->d_adj();
-    g.offT = r->d_offT();
-    g.adjT = r->d_adjT();
-    SCK(sccb::graph_features(g, feat_scratch, feat_bytes, &x[i * sccb::kFeatures], solve_st), "features");
-  }
-  std::vector<int32_t> ch(todo.size() * 3);
-  int rc = scc_mlp_predict(mlp, x.data(), (uint32_t)todo.size(), ch.data());
+  SCK(cudaStreamWaitEvent(st, r->uploaded, 0), "wait upload");
+  sccb::EngGraph g{};
+  g.n = r->g.n;
+  g.m = r->g.m;
+  g.sorted_unique = r->g.sorted_unique ? 1u : 0u;
+  g.off = r->d_off();
+  g.adj = r->d_adj();
+  g.offT = r->d_offT();
+  g.adjT = r->d_adjT();
+  float x[sccb::kFeatures];
+  SCK(sccb::graph_features(g, scratch, bytes, x, st), "features");
+  std::lock_guard<std::mutex> lk(mlp_mu);
+  int rc = scc_mlp_predict(mlp, x, 1, r->choice);
   if (rc) return rc;
-  for (size_t i = 0; i < todo.size(); ++i) {
-    std::memcpy(todo[i]->choice, &ch[i * 3], sizeof(todo[i]->choice));
-    todo[i]->have_choice = true;
+  r->have_choice = true;
+  return SCC_OK;
+}
+
+// Requests normally arrive with their choice (made by the admission thread
+// while earlier batches run); this covers any that did not.
+int scc_server::choose(std::vector<Request *> &ready) {
+  for (Request *r : ready) {
+    if (r->have_choice) continue;
+    if (!mlp) {
+      r->have_choice = true;  // plain options: choice (0,0,0)
+      continue;
+    }
+    int rc = pick(r, solve_st, feat_scratch, feat_bytes);
+    if (rc) return rc;
   }
   return SCC_OK;
 }
@@ -595,7 +613,7 @@ int scc_server_stop(scc_server *s) {
     if (r->uploaded) cudaEventDestroy(r->uploaded);
   }
   for (void *p : {(void *)s->p_off, (void *)s->p_offT, (void *)s->p_adj, (void *)s->p_adjT, (void *)s->d_labels,
-                  (void *)s->d_desc, (void *)s->d_nscc, s->feat_scratch})
+                  (void *)s->d_desc, (void *)s->d_nscc, s->feat_scratch, s->admit_scratch})
     if (p) cudaFree(p);
   if (s->mlp) scc_mlp_destroy(s->mlp);
   if (s->ctx) scc_ctx_destroy(s->ctx);
