@@ -182,45 +182,6 @@ struct Eng {
     }
   }
 
-  // Three stages over a list: the entry three iterations ahead, load1 (per-
-  // vertex words and offsets) two ahead, load2 (reads that need load1's
-  // results, e.g. the head of an adjacency list) one ahead; then f(v, valid,
-  // pre1, pre2) on the current entry.
-  template <class L1, class L2, class F>
-  __device__ void for_list_pf3(const uint32_t *lst, uint32_t cnt, L1 &&load1, L2 &&load2, F &&f) {
-    const uint32_t lim = (cnt + BS - 1u) / BS * BS;
-    const uint32_t stride = gstride();
-    uint32_t base = blockIdx.x * BS;
-    if (base >= lim) return;
-    const uint32_t i0 = base + threadIdx.x;
-    bool val0 = i0 < cnt, val1 = i0 + stride < cnt, val2 = i0 + 2u * stride < cnt;
-    uint32_t v0 = val0 ? ldm(lst + i0) : 0u;
-    uint32_t v1 = val1 ? ldm(lst + i0 + stride) : 0u;
-    uint32_t v2 = val2 ? ldm(lst + i0 + 2u * stride) : 0u;
-    auto p0 = load1(v0, val0);
-    auto p1 = load1(v1, val1);
-    auto h0 = load2(v0, val0, p0);
-    for (; base < lim; base += stride) {
-      const uint32_t i3 = base + 3u * stride + threadIdx.x;
-      const bool val3 = i3 < cnt;
-      const uint32_t v3 = val3 ? ldm(lst + i3) : 0u;
-      auto p2 = p1;
-      if (base + 2u * stride < lim) p2 = load1(v2, val2);
-      auto h1 = h0;
-      if (base + stride < lim) h1 = load2(v1, val1, p1);
-      f(v0, val0, p0, h0);
-      p0 = p1;
-      p1 = p2;
-      h0 = h1;
-      v0 = v1;
-      val0 = val1;
-      v1 = v2;
-      val1 = val2;
-      v2 = v3;
-      val2 = val3;
-    }
-  }
-
   template <class L, class F>
   __device__ void for_vertices_pf(L &&load, F &&f) {
     if (list_mode) {
@@ -590,12 +551,20 @@ struct Eng {
     }
     __syncthreads();
     uint32_t nelim = 0, nfound = 0;
-    // A: eliminate F∩B, elect pivots (CTA-local min per key, flushed below)
-    for_vertices([&](uint32_t v, bool valid) {
+    // per-vertex words and the partition id, loaded one iteration ahead (only
+    // v's own lane changes v's bits and range during either sweep)
+    struct Pre {
+      uint32_t ew, fw, bw, r;
+    };
+    auto load = [&](uint32_t v, bool valid) {
       const uint32_t w = v >> 5;
-      const uint32_t ew = ldm(s.elim + w), fw = ldm(s.fvis + w), bw = ldm(s.bvis + w);
+      return Pre{ldm(s.elim + w), ldm(s.fvis + w), ldm(s.bvis + w), ldm(s.range + (valid ? v : 0u))};
+    };
+    // A: eliminate F∩B, elect pivots (CTA-local min per key, flushed below)
+    for_vertices_pf(load, [&](uint32_t v, bool valid, const Pre &pre) {
+      const uint32_t ew = pre.ew, fw = pre.fw, bw = pre.bw;
       if (!list_mode && ~ew == 0u) return;  // whole word already eliminated
-      const uint32_t r = ldm(s.range + (valid ? v : 0u));
+      const uint32_t r = pre.r;
       uint32_t key = kNone;
       unsigned long long val = ~0ull;
       bool fb = false;
@@ -643,12 +612,13 @@ struct Eng {
     __shared__ unsigned long long s_hit[kSlotCache];  // (key << 32) | pivot
     for (int i = threadIdx.x; i < kSlotCache; i += BS) s_hit[i] = ~0ull;
     __syncthreads();
-    for_vertices([&](uint32_t v, bool valid) {
+    for_vertices_pf(load, [&](uint32_t v, bool valid, const Pre &pre) {
       bool is_piv = false;
       uint32_t key = 0;
-      if (valid && live(v)) {
-        const bool f = bit_test(s.fvis, v), b = bit_test(s.bvis, v);
-        key = 3u * ldm(s.range + v) + (f ? 1u : 0u) + (b ? 2u : 0u);
+      const uint32_t bit = 1u << (v & 31u);
+      if (valid && !(pre.ew & bit)) {
+        const bool f = pre.fw & bit, b = pre.bw & bit;
+        key = 3u * pre.r + (f ? 1u : 0u) + (b ? 2u : 0u);
         const uint32_t h = key % kSlotCache;
         const unsigned long long cached = s_hit[h];
         uint32_t np;
@@ -731,10 +701,8 @@ struct Eng {
   // four entries at a time (one 16-byte load once aligned) and the four
   // bitmap words are requested together, so a thread keeps several
   // independent L2 requests in flight instead of one dependent chain.
-  // head: the aligned 16 bytes holding adj[b] when the caller loaded them
-  // ahead (pull_head below), else nullptr.
   __device__ bool any_visited(const uint32_t *__restrict__ adj, uint32_t b, uint32_t e, const uint32_t *vis,
-                              bool ranged, uint32_t rv, const uint4 *head = nullptr) {
+                              bool ranged, uint32_t rv) {
     const uint32_t *rng = P.s.range;
     auto hit = [&](uint32_t u) {
       return ((ldm(vis + (u >> 5)) >> (u & 31u)) & 1u) && (!ranged || ldm(rng + u) == rv);
@@ -743,12 +711,12 @@ struct Eng {
     // 16-byte loads only when the list base is 16-byte aligned (caller-bound
     // graphs may not be); otherwise the scalar tail loop below does it all
     const bool vec = (reinterpret_cast<uintptr_t>(adj) & 15u) == 0;
-    if (vec && i < e && ((i & 3u) || head)) {
+    if (vec && i < e && (i & 3u)) {
       // the aligned 16 bytes holding the list head (entries of the previous
       // list masked off) instead of up to three dependent scalar probes
       const uint32_t a = i & ~3u;
       if ((unsigned long long)a + 4ull <= P.g.m) {
-        const uint4 q = head ? *head : __ldg(reinterpret_cast<const uint4 *>(adj + a));
+        const uint4 q = __ldg(reinterpret_cast<const uint4 *>(adj + a));
         const uint32_t u[4] = {q.x, q.y, q.z, q.w};
         uint32_t w[4];
 #pragma unroll
@@ -1065,40 +1033,26 @@ struct Eng {
         // list, and the next pull sweep of this reach examines only them.
         uint32_t *rem_out = rem_sel ? s.pivkey : s.aux;
         Stage rq{rem_out, cur() + C_REM, s.qcap, 0, stage_buf(1)};
-        auto body = [&](uint32_t v, bool valid, const Pre &p, bool aligned, const uint4 *head) {
+        auto body = [&](uint32_t v, bool valid, const Pre &p, bool aligned) {
           // whole warp = one bitmap word in full mode: skip words without a live unvisited vertex
           if (aligned && (~p.vw & ~p.ew) == 0u) return;
           bool found = false;
           const bool cand = valid && !(((p.vw | p.ew) >> (v & 31u)) & 1u);
           if (cand) {
-            found = any_visited(padj, p.pb, p.pe, vis, ranged, p.rv, head);
+            found = any_visited(padj, p.pb, p.pe, vis, ranged, p.rv);
             if (found) degsum += p.pe - p.pb;
           }
           warp_set_bits(vis, v, found, aligned);
           stage_put(pq, found, v);
           stage_put(rq, cand && !found, v);
         };
-        // list sweeps also load each candidate's list head one entry ahead
-        const bool head_ok = (reinterpret_cast<uintptr_t>(padj) & 15u) == 0;
-        auto head = [&](uint32_t v, bool valid, const Pre &p) {
-          uint4 q = make_uint4(0u, 0u, 0u, 0u);
-          const bool cand = valid && !(((p.vw | p.ew) >> (v & 31u)) & 1u);
-          const uint32_t a = p.pb & ~3u;
-          if (head_ok && cand && p.pe > p.pb && (unsigned long long)a + 4ull <= P.g.m)
-            q = __ldg(reinterpret_cast<const uint4 *>(padj + a));
-          return q;
-        };
-        auto list_body = [&](uint32_t v, bool valid, const Pre &p, const uint4 &q) {
-          const uint32_t a = p.pb & ~3u;
-          const bool have = head_ok && p.pe > p.pb && (unsigned long long)a + 4ull <= P.g.m;
-          body(v, valid, p, false, have ? &q : nullptr);
-        };
         if (rem_valid) {
-          for_list_pf3(rem_in, rem_n, load, head, list_body);
+          for_list_pf(rem_in, rem_n, load, [&](uint32_t v, bool valid, const Pre &p) { body(v, valid, p, false); });
         } else if (list_mode) {
-          for_list_pf3(s.act[act_sel], act_count, load, head, list_body);
+          for_list_pf(s.act[act_sel], act_count, load,
+                      [&](uint32_t v, bool valid, const Pre &p) { body(v, valid, p, false); });
         } else {
-          for_vertices_pf(load, [&](uint32_t v, bool valid, const Pre &p) { body(v, valid, p, true, nullptr); });
+          for_vertices_pf(load, [&](uint32_t v, bool valid, const Pre &p) { body(v, valid, p, true); });
         }
         stage_flush(pq);
         stage_flush(rq);
@@ -1345,31 +1299,35 @@ struct Eng {
     if (!list_mode) {
       // one bitmap word per lane (ids 0 and > n are marked eliminated at
       // init): a warp covers 1024 ids per step, scans its live counts and
-      // appends them with one atomicAdd, each lane its word's ids in order
+      // appends them with one atomicAdd; then word by word, the lanes whose
+      // bit is set write that word's ids side by side (coalesced stores)
       const uint32_t lane = lane_id();
       for (uint32_t w0 = gwarp() * 32u; w0 < s.nwords; w0 += nwarps() * 32u) {
         const uint32_t w = w0 + lane;
-        uint32_t live = w < s.nwords ? ~ldm(s.elim + w) : 0u;
+        const uint32_t live = w < s.nwords ? ~ldm(s.elim + w) : 0u;
         const uint32_t cnt = __popc(live);
         const uint32_t incl = warp_incl_scan(cnt);
         uint32_t base = 0;
         if (lane == 31 && incl) base = atomicAdd(cur() + C_Q, incl);
         base = __shfl_sync(kFull, base, 31);
-        uint32_t pos = base + incl - cnt;
-        while (live) {
-          const uint32_t b = __ffs(live) - 1u;
-          if (pos < s.qcap) dst[pos] = w * 32u + b;
-          else fail(kErrQueueOverflow);
-          ++pos;
-          live &= live - 1u;
+        const uint32_t pos = base + incl - cnt;
+        for (uint32_t j = 0; j < 32u; ++j) {
+          const uint32_t lj = __shfl_sync(kFull, live, j);
+          if (lj == 0u) continue;
+          const uint32_t pj = __shfl_sync(kFull, pos, j);
+          if ((lj >> lane) & 1u) {
+            const uint32_t at = pj + __popc(lj & lanemask_lt());
+            if (at < s.qcap) dst[at] = (w0 + j) * 32u + lane;
+            else fail(kErrQueueOverflow);
+          }
         }
       }
     } else {
       Stage aq{dst, cur() + C_Q, s.qcap, 0, stage_buf()};
-      for_vertices([&](uint32_t v, bool valid) {
-        const uint32_t ew = ldm(s.elim + (v >> 5));
-        stage_put(aq, valid && !((ew >> (v & 31u)) & 1u), v);
-      });
+      for_vertices_pf([&](uint32_t v, bool) { return ldm(s.elim + (v >> 5)); },
+                      [&](uint32_t v, bool valid, uint32_t ew) {
+                        stage_put(aq, valid && !((ew >> (v & 31u)) & 1u), v);
+                      });
       stage_flush(aq);
     }
     if (!bar(1000)) return;

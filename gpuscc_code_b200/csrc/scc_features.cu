@@ -186,10 +186,11 @@ size_t features_scratch_bytes(uint32_t n) {
   return sizeof(FeatAcc) + words * 4 + 2 * ((size_t)n + 1) * 4 + 64;
 }
 
-cudaError_t graph_features(const EngGraph &g, void *scratch, size_t scratch_bytes, float *feat,
-                           cudaStream_t st) {
-  std::memset(feat, 0, sizeof(float) * kFeatures);
-  if (g.n == 0) return cudaSuccess;
+size_t features_acc_bytes() { return sizeof(FeatAcc); }
+
+cudaError_t graph_features_launch(const EngGraph &g, void *scratch, size_t scratch_bytes, void *host_acc,
+                                  cudaStream_t st) {
+  if (g.n == 0) return cudaSuccess;  // graph_features_finish gives zeros
   if (scratch_bytes < features_scratch_bytes(g.n)) return cudaErrorInvalidValue;
   const size_t words = ((size_t)g.n + 32) / 32 + 4;
   FeatAcc *acc = reinterpret_cast<FeatAcc *>(scratch);
@@ -207,11 +208,24 @@ cudaError_t graph_features(const EngGraph &g, void *scratch, size_t scratch_byte
   bfs_level_kernel<<<148 * 8, 256, 0, st>>>(g, lb, &acc->lvl[1], la, &acc->lvl[2], vis);
   bfs_level_kernel<<<148 * 8, 256, 0, st>>>(g, la, &acc->lvl[2], lb, &acc->lvl[3], vis);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
-  FeatAcc h;
-  if ((e = cudaMemcpyAsync(&h, acc, sizeof(FeatAcc), cudaMemcpyDeviceToHost, st)) != cudaSuccess) return e;
-  if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return e;
-  features_from_counts(g.n, g.m, h.sum_out, h.sumsq_out, h.max_out, h.max_in, h.z_out, h.z_in, h.z_any,
-                       h.one_out, h.one_in, h.low, h.recip, h.recip_n, h.lvl, feat);
+  return cudaMemcpyAsync(host_acc, acc, sizeof(FeatAcc), cudaMemcpyDeviceToHost, st);
+}
+
+void graph_features_finish(uint32_t n, uint32_t m, const void *host_acc, float *feat) {
+  std::memset(feat, 0, sizeof(float) * kFeatures);
+  if (n == 0) return;
+  const FeatAcc &h = *reinterpret_cast<const FeatAcc *>(host_acc);
+  features_from_counts(n, m, h.sum_out, h.sumsq_out, h.max_out, h.max_in, h.z_out, h.z_in, h.z_any, h.one_out,
+                       h.one_in, h.low, h.recip, h.recip_n, h.lvl, feat);
+}
+
+cudaError_t graph_features(const EngGraph &g, void *scratch, size_t scratch_bytes, float *feat,
+                           cudaStream_t st) {
+  FeatAcc h{};
+  cudaError_t e = graph_features_launch(g, scratch, scratch_bytes, &h, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return e;
+  graph_features_finish(g.n, g.m, &h, feat);
   return cudaSuccess;
 }
 

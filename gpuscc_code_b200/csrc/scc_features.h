@@ -21,6 +21,14 @@ size_t features_scratch_bytes(uint32_t n);
 // f[12] sampled reciprocity, f[13..15] log2(1+|BFS level k|)/log2(n+1) for
 // k = 1..3 from the vertex of largest total degree.
 cudaError_t graph_features(const EngGraph &g, void *scratch, size_t scratch_bytes, float *feat, cudaStream_t st);
+// The same in two halves: launch enqueues the kernels and the copy of the
+// accumulators (features_acc_bytes of them) to host_acc (page-locked) on st
+// without waiting; finish forms the features from host_acc once st has
+// passed that point.  scratch may be released (stream-ordered) right after.
+size_t features_acc_bytes();
+cudaError_t graph_features_launch(const EngGraph &g, void *scratch, size_t scratch_bytes, void *host_acc,
+                                  cudaStream_t st);
+void graph_features_finish(uint32_t n, uint32_t m, const void *host_acc, float *feat);
 void features_from_counts(uint32_t n, uint32_t m, unsigned long long sum_out, double sumsq_out, uint32_t max_out,
                           uint32_t max_in, uint32_t z_out, uint32_t z_in, uint32_t z_any, uint32_t one_out,
                           uint32_t one_in, uint32_t low, uint32_t recip, uint32_t recip_n, const uint32_t lvl[4],

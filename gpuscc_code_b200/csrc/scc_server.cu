@@ -91,6 +91,8 @@ struct Request {
   cudaEvent_t uploaded = nullptr;
   bool have_choice = false;
   int32_t choice[3] = {0, 0, 0};
+  void *h_acc = nullptr;  // page-locked slot receiving the feature accumulators
+  bool feat_pending = false;
   scc_request_info info{};
   const uint32_t *d_off() const { return static_cast<const uint32_t *>(dmem); }
   const uint32_t *d_offT() const { return d_off() + pad4(g.n + 2); }
@@ -117,8 +119,6 @@ struct scc_server {
   uint32_t labels_cap = 0;
   PackDesc *d_desc = nullptr;
   uint32_t *d_nscc = nullptr;
-  void *feat_scratch = nullptr;
-  size_t feat_bytes = 0;
   scc_mlp *mlp = nullptr;
 
   std::mutex mu;
@@ -135,10 +135,11 @@ struct scc_server {
   void solve_loop();
   int run_batch(std::vector<Request *> &batch);
   int choose(std::vector<Request *> &ready);
-  int pick(Request *r, cudaStream_t st, void *&scratch, size_t &bytes);
-  std::mutex mlp_mu;                  // the network's buffers are shared by both threads
-  void *admit_scratch = nullptr;      // feature scratch of the admission thread
-  size_t admit_bytes = 0;
+  // page-locked slots for feature accumulators (one per request in flight)
+  std::mutex acc_mu;
+  std::vector<void *> acc_free, acc_chunks;
+  void *get_acc();
+  void put_acc(void *p);
   void finish(Request *r, int status);
 };
 
@@ -183,21 +184,32 @@ void scc_server::admit_loop() {
         e = cudaMemcpyAsync(const_cast<uint32_t *>(r->d_adj()), r->g.edges, mb, cudaMemcpyHostToDevice, copy_st);
       if (e == cudaSuccess && mb)
         e = cudaMemcpyAsync(const_cast<uint32_t *>(r->d_adjT()), r->g.edgesT, mb, cudaMemcpyHostToDevice, copy_st);
+      // with a network loaded, the graph's features are computed on the copy
+      // stream behind the upload, with nothing waiting for them: the solver
+      // reads the accumulators when it forms the batch that may take r
+      if (e == cudaSuccess && mlp) {
+        void *scratch = nullptr;
+        const size_t fb = sccb::features_scratch_bytes(r->g.n);
+        r->h_acc = get_acc();
+        e = r->h_acc ? cudaMallocFromPoolAsync(&scratch, fb, pool, copy_st) : cudaErrorMemoryAllocation;
+        if (e == cudaSuccess) {
+          sccb::EngGraph g{};
+          g.n = r->g.n;
+          g.m = r->g.m;
+          g.sorted_unique = r->g.sorted_unique ? 1u : 0u;
+          g.off = r->d_off();
+          g.adj = r->d_adj();
+          g.offT = r->d_offT();
+          g.adjT = r->d_adjT();
+          e = sccb::graph_features_launch(g, scratch, fb, r->h_acc, copy_st);
+          cudaFreeAsync(scratch, copy_st);
+          r->feat_pending = e == cudaSuccess;
+        }
+      }
       if (e == cudaSuccess) e = cudaEventCreateWithFlags(&r->uploaded, cudaEventDisableTiming);
       if (e == cudaSuccess) e = cudaEventRecord(r->uploaded, copy_st);
     }
-    // with a network loaded, pick this request's options now, while earlier
-    // batches run (features run on the copy stream after the upload)
-    int prc = SCC_OK;
-    if (e == cudaSuccess && mlp) prc = pick(r, copy_st, admit_scratch, admit_bytes);
     lk.lock();
-    if (e == cudaSuccess && prc != SCC_OK) {
-      lk.unlock();
-      cudaStreamSynchronize(copy_st);
-      finish(r, prc);
-      lk.lock();
-      continue;
-    }
     if (e != cudaSuccess) {
       sccb::set_error(SCC_ERR_CUDA, "upload: %s", cudaGetErrorString(e));
       cudaStreamSynchronize(copy_st);  // nothing may still write into the allocation when it is freed
@@ -215,6 +227,11 @@ void scc_server::admit_loop() {
 // after the solve stream's work) and wakes waiters.
 void scc_server::finish(Request *r, int status) {
   if (r->uploaded) cudaStreamWaitEvent(solve_st, r->uploaded, 0);  // the upload may still be in flight
+  if (r->h_acc) {
+    if (r->uploaded) cudaEventSynchronize(r->uploaded);  // the accumulator copy lands in the slot
+    put_acc(r->h_acc);
+    r->h_acc = nullptr;
+  }
   if (r->dmem) cudaFreeAsync(r->dmem, solve_st);
   r->dmem = nullptr;
   if (r->uploaded) cudaEventDestroy(r->uploaded);
@@ -233,46 +250,53 @@ void scc_server::finish(Request *r, int status) {
 }
 
 // Features + network choice for the ready requests that have none yet.
-// Features of r's resident graph on stream st (ordered after its upload),
-// then the network's choice.  Scratch is the caller's (one per thread).
-int scc_server::pick(Request *r, cudaStream_t st, void *&scratch, size_t &bytes) {
-  const size_t need = sccb::features_scratch_bytes(r->g.n);
-  if (need > bytes) {
-    if (scratch) cudaFree(scratch);
-    scratch = nullptr;
-    bytes = 0;
-    SCK(cudaMalloc(&scratch, need), "alloc feature scratch");
-    bytes = need;
+void *scc_server::get_acc() {
+  std::lock_guard<std::mutex> lk(acc_mu);
+  if (acc_free.empty()) {
+    constexpr size_t kSlot = 256, kSlots = 256;
+    void *chunk = nullptr;
+    if (cudaMallocHost(&chunk, kSlot * kSlots) != cudaSuccess) return nullptr;
+    acc_chunks.push_back(chunk);
+    for (size_t i = 0; i < kSlots; ++i) acc_free.push_back(static_cast<char *>(chunk) + i * kSlot);
   }
-  SCK(cudaStreamWaitEvent(st, r->uploaded, 0), "wait upload");
-  sccb::EngGraph g{};
-  g.n = r->g.n;
-  g.m = r->g.m;
-  g.sorted_unique = r->g.sorted_unique ? 1u : 0u;
-  g.off = r->d_off();
-  g.adj = r->d_adj();
-  g.offT = r->d_offT();
-  g.adjT = r->d_adjT();
-  float x[sccb::kFeatures];
-  SCK(sccb::graph_features(g, scratch, bytes, x, st), "features");
-  std::lock_guard<std::mutex> lk(mlp_mu);
-  int rc = scc_mlp_predict(mlp, x, 1, r->choice);
-  if (rc) return rc;
-  r->have_choice = true;
-  return SCC_OK;
+  void *p = acc_free.back();
+  acc_free.pop_back();
+  return p;
 }
 
-// Requests normally arrive with their choice (made by the admission thread
-// while earlier batches run); this covers any that did not.
+void scc_server::put_acc(void *p) {
+  if (!p) return;
+  std::lock_guard<std::mutex> lk(acc_mu);
+  acc_free.push_back(p);
+}
+
+// Choices for the ready requests that have none: their features were
+// launched at admission; one forward pass of the network covers them all.
+// Without a network (or without features) a request keeps choice (0,0,0),
+// the plain method.
 int scc_server::choose(std::vector<Request *> &ready) {
+  std::vector<Request *> todo;
   for (Request *r : ready) {
     if (r->have_choice) continue;
-    if (!mlp) {
-      r->have_choice = true;  // plain options: choice (0,0,0)
+    if (!mlp || !r->feat_pending) {
+      r->have_choice = true;
       continue;
     }
-    int rc = pick(r, solve_st, feat_scratch, feat_bytes);
-    if (rc) return rc;
+    todo.push_back(r);
+  }
+  if (todo.empty()) return SCC_OK;
+  std::vector<float> x(todo.size() * sccb::kFeatures);
+  for (size_t i = 0; i < todo.size(); ++i) {
+    Request *r = todo[i];
+    SCK(cudaEventSynchronize(r->uploaded), "features");
+    sccb::graph_features_finish(r->g.n, r->g.m, r->h_acc, &x[i * sccb::kFeatures]);
+  }
+  std::vector<int32_t> ch(todo.size() * 3);
+  int rc = scc_mlp_predict(mlp, x.data(), (uint32_t)todo.size(), ch.data());
+  if (rc) return rc;
+  for (size_t i = 0; i < todo.size(); ++i) {
+    std::memcpy(todo[i]->choice, &ch[i * 3], sizeof(todo[i]->choice));
+    todo[i]->have_choice = true;
   }
   return SCC_OK;
 }
@@ -448,6 +472,7 @@ int scc_server_start(const scc_server_cfg *cfg, scc_server **out) {
   if (!s->cfg.max_batch_edges) s->cfg.max_batch_edges = 1u << 27;
   if (!s->cfg.solo_vertices) s->cfg.solo_vertices = 1u << 18;
   if (s->cfg.max_batch_vertices >= (1u << 30)) return sccb::set_error(SCC_ERR_INVALID, "max_batch_vertices >= 2^30");
+  if (sccb::features_acc_bytes() > 256) return sccb::set_error(SCC_ERR_STATE, "feature accumulator slot too small");
   SCK(cudaSetDevice(cfg->device), "cudaSetDevice");
   int rc = scc_ctx_create(cfg->device, &cfg->opts, &s->ctx);
   if (rc) return rc;
@@ -613,8 +638,9 @@ int scc_server_stop(scc_server *s) {
     if (r->uploaded) cudaEventDestroy(r->uploaded);
   }
   for (void *p : {(void *)s->p_off, (void *)s->p_offT, (void *)s->p_adj, (void *)s->p_adjT, (void *)s->d_labels,
-                  (void *)s->d_desc, (void *)s->d_nscc, s->feat_scratch, s->admit_scratch})
+                  (void *)s->d_desc, (void *)s->d_nscc})
     if (p) cudaFree(p);
+  for (void *c : s->acc_chunks) cudaFreeHost(c);
   if (s->mlp) scc_mlp_destroy(s->mlp);
   if (s->ctx) scc_ctx_destroy(s->ctx);
   if (s->copy_st) cudaStreamDestroy(s->copy_st);
