@@ -599,6 +599,69 @@ def run_serve(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+def run_refgpu(args) -> None:
+    """The reference's own GPU FB (scc_2_w build, compiled from its sources for
+    sm_100a into oracle/_ref) against this engine on the same graphs and the
+    same device: R-MAT scale 16 / 2^20 samples (seed 1, config 1), R-MAT at
+    larger scales (seed 2) and a grid.  The reference runs in a child process
+    (it prints and exit()s on errors) under a time limit; both sides report the
+    solve time from a resident CSR (the reference's own timer, scc.cu:217-1011;
+    CUDA events here) and the SCC count, which must agree."""
+    import subprocess
+
+    import torch
+
+    import gpuscc_code_b200 as scc
+    from oracle import ref_gpu
+
+    if not ref_gpu.available():
+        print(json.dumps({"metric": "reference GPU FB comparison", "unavailable": "oracle/_ref/libscc_ref_gpu.so "
+                          "not built (the reference sources were absent at build time)"}))
+        return
+    torch.cuda.set_device(0)
+    cases = [("rmat16_e20_seed1", ["--rmat", "16", "--samples-log2", "20", "--seed", "1"],
+              lambda c: c.gen_rmat_device(16, 1 << 20, seed=1))]
+    for sc in args.refgpu_scales:
+        cases.append((f"rmat{sc}_e{sc + 4}_seed2", ["--rmat", str(sc), "--samples-log2", str(sc + 4), "--seed", "2"],
+                      lambda c, sc=sc: c.gen_rmat_device(sc, 1 << (sc + 4), seed=2)))
+    cases.append((f"grid{args.refgpu_grid}_seed3", ["--grid", str(args.refgpu_grid), "--seed", "3"], None))
+    rows = []
+    for name, cli, gen in cases:
+        row = {"graph": name}
+        for alg in args.refgpu_algs:
+            try:
+                r = subprocess.run([sys.executable, "-m", "oracle.ref_gpu", *cli, "--alg", alg], cwd=ROOT,
+                                   capture_output=True, text=True, timeout=args.refgpu_timeout)
+                ref = json.loads(r.stdout.strip().splitlines()[-1]) if r.returncode == 0 else {
+                    "error": f"exit {r.returncode}: {(r.stderr or r.stdout).strip()[-200:]}"}
+            except subprocess.TimeoutExpired:
+                ref = {"error": f"no result within {args.refgpu_timeout} s"}
+            row[f"reference_{alg}"] = ref
+        ctx = scc.SCCContext(0, scc.Options(alg="h", wcc=True, trim2=True))
+        if gen is None:
+            ctx.upload(scc.gen_grid(args.refgpu_grid, 0.15, 0.001, seed=3))
+        else:
+            gen(ctx)
+        for _ in range(3):
+            cnt, st = ctx.solve_device()
+        ms = []
+        for _ in range(5):
+            cnt, st = ctx.solve_device()
+            ms.append(st["ms_total"])
+        ctx.close()
+        row["ours_h"] = {"n": ctx.n, "nscc": cnt, "secs": statistics.median(ms) / 1e3}
+        for alg in args.refgpu_algs:
+            ref = row[f"reference_{alg}"]
+            if "secs" in ref:
+                ref["count_matches"] = ref["nscc"] == cnt
+                ref["speedup_of_ours"] = ref["secs"] / row["ours_h"]["secs"]
+        rows.append(row)
+    print(json.dumps({"metric": "SCC solve time vs the reference's GPU FB (same B200, same graphs)",
+                      "unit": "s", "rows": rows,
+                      "note": "reference: scc.cu computeSCC of the scc_2_w build (-DWCC -DTRIM_2), its own timer; "
+                              "ours: scc_2_w -a h, CUDA events, median of 5"}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -617,7 +680,12 @@ def main():
     ap.add_argument("--opt", action="append", default=[], metavar="KEY=VALUE",
                     help="override an engine option (scc_opts field), e.g. --opt occupancy=3")
     ap.add_argument("--grid-side", type=int, default=4096, help="grid: side of the grid graph")
-    ap.add_argument("--workload", choices=["rmat26", "grid", "batch", "serve"], default="rmat26",
+    ap.add_argument("--refgpu-scales", type=int, nargs="*", default=[20, 22],
+                    help="refgpu: further R-MAT scales (2^(scale+4) samples, seed 2)")
+    ap.add_argument("--refgpu-grid", type=int, default=1024, help="refgpu: grid side")
+    ap.add_argument("--refgpu-algs", nargs="*", default=["h", "t"], help="refgpu: reference -a arms")
+    ap.add_argument("--refgpu-timeout", type=int, default=300)
+    ap.add_argument("--workload", choices=["rmat26", "grid", "batch", "serve", "refgpu"], default="rmat26",
                     help="rmat26: the headline line; batch: 4096 packed graphs in one launch vs one launch each; "
                          "serve: Poisson stream through the request loop (plain / batched / batched + network); "
                          "grid: the 4096^2 high-diameter grid graph")
@@ -630,6 +698,12 @@ def main():
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if args.workload == "refgpu":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "the refgpu workload is itself a comparison"}))
+            return
+        run_refgpu(args)
+        return
     if args.workload in ("batch", "serve"):
         if args.impl == "reference":
             print(json.dumps({"impl": "reference",
