@@ -310,8 +310,10 @@ struct Eng {
     const uint32_t lane = lane_id();
     const bool vec = ((reinterpret_cast<uintptr_t>(g.off) | reinterpret_cast<uintptr_t>(g.offT)) & 15u) == 0;
     const uint32_t step = gstride() * 4u;
+    // stage 1: offsets of four ids (lane 31 also the fifth, which the other
+    // lanes take from their right neighbour)
     struct Quad {
-      uint32_t o[4], t[4];
+      uint32_t o[4], t[4], o4, t4;
     };
     auto load = [&](uint32_t v0) {
       Quad q;
@@ -328,43 +330,56 @@ struct Eng {
           q.t[i] = in ? ldg(g.offT + v0 + i) : 0u;
         }
       }
+      const bool in4 = lane == 31 && v0 + 4u <= n + 1u;
+      q.o4 = in4 ? ldg(g.off + v0 + 4u) : 0u;
+      q.t4 = in4 ? ldg(g.offT + v0 + 4u) : 0u;
       return q;
+    };
+    // stage 2: degree classes, and the heads of single-entry lists (self-
+    // loop test) where the other direction does not already decide
+    struct Heads {
+      uint32_t x[4], y[4];
+      uint32_t code;  // per id i, bits 4i..4i+3: out-degree 0, in-degree 0, out-degree 1, in-degree 1
+    };
+    auto heads = [&](uint32_t v0, const Quad &q) {
+      Heads h;
+      const uint32_t so = __shfl_down_sync(kFull, q.o[0], 1), st = __shfl_down_sync(kFull, q.t[0], 1);
+      const uint32_t o4 = lane == 31 ? q.o4 : so, t4 = lane == 31 ? q.t4 : st;
+      h.code = 0;
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const uint32_t dout = (i < 3 ? q.o[i + 1] : o4) - q.o[i];
+        const uint32_t din = (i < 3 ? q.t[i + 1] : t4) - q.t[i];
+        const bool valid = v0 + i >= 1u && v0 + i <= n;
+        const bool open = valid && dout != 0 && din != 0;
+        h.x[i] = (open && dout == 1) ? ldg(g.adj + q.o[i]) : 0u;
+        h.y[i] = (open && din == 1) ? ldg(g.adjT + q.t[i]) : 0u;
+        h.code |= ((dout == 0 ? 1u : 0u) | (din == 0 ? 2u : 0u) | (dout == 1 ? 4u : 0u) | (din == 1 ? 8u : 0u))
+                  << (4 * i);
+      }
+      return h;
     };
     uint32_t ntrim = 0;
     uint32_t base = blockIdx.x * BS * 4u;
     const uint32_t wofs = (threadIdx.x >> 5) * 128u + lane * 4u;
     if (base >= lim) return 0;
-    Quad cur_q = load(base + wofs);
+    // loads run two iterations ahead, list heads one
+    Quad q1 = load(base + wofs);
+    Heads h0 = heads(base + wofs, q1);
+    if (base + step < lim) q1 = load(base + step + wofs);
     for (; base < lim; base += step) {
       const uint32_t v0 = base + wofs;
-      // next iteration's offsets are in flight while this one is decided
-      Quad nxt = cur_q;
-      if (base + step < lim) nxt = load(base + step + wofs);
-      const Quad &q = cur_q;
-      uint32_t o4 = __shfl_down_sync(kFull, q.o[0], 1), t4 = __shfl_down_sync(kFull, q.t[0], 1);
-      if (lane == 31) {
-        const bool in = v0 + 4u <= n + 1u;
-        o4 = in ? ldg(g.off + v0 + 4u) : 0u;
-        t4 = in ? ldg(g.offT + v0 + 4u) : 0u;
-      }
-      // degrees first; the single-entry lists' heads (self-loop test) are
-      // loaded together, and only where the other direction does not decide
-      uint32_t dout[4], din[4], x[4], y[4];
-#pragma unroll
-      for (int i = 0; i < 4; ++i) {
-        dout[i] = (i < 3 ? q.o[i + 1] : o4) - q.o[i];
-        din[i] = (i < 3 ? q.t[i + 1] : t4) - q.t[i];
-        const bool valid = v0 + i >= 1u && v0 + i <= n;
-        const bool open = valid && dout[i] != 0 && din[i] != 0;
-        x[i] = (open && dout[i] == 1) ? ldg(g.adj + q.o[i]) : 0u;
-        y[i] = (open && din[i] == 1) ? ldg(g.adjT + q.t[i]) : 0u;
-      }
+      Quad q2 = q1;
+      if (base + 2u * step < lim) q2 = load(base + 2u * step + wofs);
+      Heads h1 = h0;
+      if (base + step < lim) h1 = heads(v0 + step, q1);
       uint32_t bits = 0;
 #pragma unroll
       for (int i = 0; i < 4; ++i) {
         const uint32_t v = v0 + i;
         if (v < 1u || v > n) continue;
-        const bool tr = dout[i] == 0 || din[i] == 0 || (dout[i] == 1 && x[i] == v) || (din[i] == 1 && y[i] == v);
+        const uint32_t c = (h0.code >> (4 * i)) & 15u;
+        const bool tr = (c & 3u) != 0 || ((c & 4u) && h0.x[i] == v) || ((c & 8u) && h0.y[i] == v);
         if (tr) {
           s.label[v] = v;
           bits |= 1u << i;
@@ -382,7 +397,8 @@ struct Eng {
         atomicOr(s.elim + w, word);
         atomicOr(s.tflag + w, word);
       }
-      cur_q = nxt;
+      h0 = h1;
+      q1 = q2;
     }
     return ntrim;
   }

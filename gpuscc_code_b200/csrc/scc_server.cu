@@ -93,6 +93,7 @@ struct Request {
   int32_t choice[3] = {0, 0, 0};
   void *h_acc = nullptr;  // page-locked slot receiving the feature accumulators
   bool feat_pending = false;
+  cudaEvent_t featured = nullptr;  // features of this request done (feature stream)
   scc_request_info info{};
   const uint32_t *d_off() const { return static_cast<const uint32_t *>(dmem); }
   const uint32_t *d_offT() const { return d_off() + pad4(g.n + 2); }
@@ -112,6 +113,7 @@ struct scc_server {
   scc_server_cfg cfg{};
   scc_ctx *ctx = nullptr;
   cudaStream_t solve_st = nullptr, copy_st = nullptr;
+  cudaStream_t feat_st = nullptr;  // feature passes: behind their upload, never in front of the next one
   cudaMemPool_t pool = nullptr;
   // packed batch CSR and its scratch
   uint32_t *p_off = nullptr, *p_offT = nullptr, *p_adj = nullptr, *p_adjT = nullptr;
@@ -184,14 +186,18 @@ void scc_server::admit_loop() {
         e = cudaMemcpyAsync(const_cast<uint32_t *>(r->d_adj()), r->g.edges, mb, cudaMemcpyHostToDevice, copy_st);
       if (e == cudaSuccess && mb)
         e = cudaMemcpyAsync(const_cast<uint32_t *>(r->d_adjT()), r->g.edgesT, mb, cudaMemcpyHostToDevice, copy_st);
-      // with a network loaded, the graph's features are computed on the copy
-      // stream behind the upload, with nothing waiting for them: the solver
-      // reads the accumulators when it forms the batch that may take r
+      if (e == cudaSuccess) e = cudaEventCreateWithFlags(&r->uploaded, cudaEventDisableTiming);
+      if (e == cudaSuccess) e = cudaEventRecord(r->uploaded, copy_st);
+      // with a network loaded, the graph's features are computed on their own
+      // stream behind the upload, with nothing waiting for them (the next
+      // uploads go on): the solver reads the accumulators when it forms the
+      // batch that may take r
       if (e == cudaSuccess && mlp) {
         void *scratch = nullptr;
         const size_t fb = sccb::features_scratch_bytes(r->g.n);
         r->h_acc = get_acc();
-        e = r->h_acc ? cudaMallocFromPoolAsync(&scratch, fb, pool, copy_st) : cudaErrorMemoryAllocation;
+        e = r->h_acc ? cudaStreamWaitEvent(feat_st, r->uploaded, 0) : cudaErrorMemoryAllocation;
+        if (e == cudaSuccess) e = cudaMallocFromPoolAsync(&scratch, fb, pool, feat_st);
         if (e == cudaSuccess) {
           sccb::EngGraph g{};
           g.n = r->g.n;
@@ -201,18 +207,19 @@ void scc_server::admit_loop() {
           g.adj = r->d_adj();
           g.offT = r->d_offT();
           g.adjT = r->d_adjT();
-          e = sccb::graph_features_launch(g, scratch, fb, r->h_acc, copy_st);
-          cudaFreeAsync(scratch, copy_st);
+          e = sccb::graph_features_launch(g, scratch, fb, r->h_acc, feat_st);
+          cudaFreeAsync(scratch, feat_st);
+          if (e == cudaSuccess) e = cudaEventCreateWithFlags(&r->featured, cudaEventDisableTiming);
+          if (e == cudaSuccess) e = cudaEventRecord(r->featured, feat_st);
           r->feat_pending = e == cudaSuccess;
         }
       }
-      if (e == cudaSuccess) e = cudaEventCreateWithFlags(&r->uploaded, cudaEventDisableTiming);
-      if (e == cudaSuccess) e = cudaEventRecord(r->uploaded, copy_st);
     }
     lk.lock();
     if (e != cudaSuccess) {
       sccb::set_error(SCC_ERR_CUDA, "upload: %s", cudaGetErrorString(e));
       cudaStreamSynchronize(copy_st);  // nothing may still write into the allocation when it is freed
+      cudaStreamSynchronize(feat_st);
       lk.unlock();
       finish(r, e == cudaErrorMemoryAllocation ? SCC_ERR_NOMEM : SCC_ERR_CUDA);
       lk.lock();
@@ -227,11 +234,14 @@ void scc_server::admit_loop() {
 // after the solve stream's work) and wakes waiters.
 void scc_server::finish(Request *r, int status) {
   if (r->uploaded) cudaStreamWaitEvent(solve_st, r->uploaded, 0);  // the upload may still be in flight
+  if (r->featured) cudaStreamWaitEvent(solve_st, r->featured, 0);  // and the feature pass reading the graph
   if (r->h_acc) {
-    if (r->uploaded) cudaEventSynchronize(r->uploaded);  // the accumulator copy lands in the slot
+    if (r->featured) cudaEventSynchronize(r->featured);  // the accumulator copy lands in the slot
     put_acc(r->h_acc);
     r->h_acc = nullptr;
   }
+  if (r->featured) cudaEventDestroy(r->featured);
+  r->featured = nullptr;
   if (r->dmem) cudaFreeAsync(r->dmem, solve_st);
   r->dmem = nullptr;
   if (r->uploaded) cudaEventDestroy(r->uploaded);
@@ -288,7 +298,7 @@ int scc_server::choose(std::vector<Request *> &ready) {
   std::vector<float> x(todo.size() * sccb::kFeatures);
   for (size_t i = 0; i < todo.size(); ++i) {
     Request *r = todo[i];
-    SCK(cudaEventSynchronize(r->uploaded), "features");
+    SCK(cudaEventSynchronize(r->featured), "features");
     sccb::graph_features_finish(r->g.n, r->g.m, r->h_acc, &x[i * sccb::kFeatures]);
   }
   std::vector<int32_t> ch(todo.size() * 3);
@@ -484,6 +494,7 @@ int scc_server_start(const scc_server_cfg *cfg, scc_server **out) {
     return code;
   };
   cudaError_t e = cudaStreamCreateWithFlags(&s->copy_st, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->feat_st, cudaStreamNonBlocking);
   cudaMemPoolProps props{};
   props.allocType = cudaMemAllocationTypePinned;
   props.location.type = cudaMemLocationTypeDevice;
@@ -632,10 +643,12 @@ int scc_server_stop(scc_server *s) {
   cudaSetDevice(s->cfg.device);
   if (s->solve_st) cudaStreamSynchronize(s->solve_st);
   if (s->copy_st) cudaStreamSynchronize(s->copy_st);
+  if (s->feat_st) cudaStreamSynchronize(s->feat_st);
   for (auto &kv : s->reqs) {
     Request *r = kv.second.get();
     if (r->dmem) cudaFree(r->dmem);
     if (r->uploaded) cudaEventDestroy(r->uploaded);
+    if (r->featured) cudaEventDestroy(r->featured);
   }
   for (void *p : {(void *)s->p_off, (void *)s->p_offT, (void *)s->p_adj, (void *)s->p_adjT, (void *)s->d_labels,
                   (void *)s->d_desc, (void *)s->d_nscc})
@@ -644,6 +657,7 @@ int scc_server_stop(scc_server *s) {
   if (s->mlp) scc_mlp_destroy(s->mlp);
   if (s->ctx) scc_ctx_destroy(s->ctx);
   if (s->copy_st) cudaStreamDestroy(s->copy_st);
+  if (s->feat_st) cudaStreamDestroy(s->feat_st);
   if (s->pool) cudaMemPoolDestroy(s->pool);
   delete s;
   return SCC_OK;
