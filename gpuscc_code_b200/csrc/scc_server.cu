@@ -13,8 +13,10 @@
 //    single graph is bound in place), runs one persistent solve, unpacks each
 //    segment's labels back to local ids and copies them to the caller's
 //    buffer, then frees the request's device memory.
-// With a strategy network loaded, the solver computes each ready request's
-// features on the device and lets the network pick its options.
+// With a strategy network loaded, the admission thread also launches each
+// request's feature pass on a stream of its own (behind the upload, never in
+// front of the next one); the solver reads the features when it forms a
+// batch and lets the network pick the options of all new requests at once.
 #include <cuda_runtime.h>
 
 #include <algorithm>
