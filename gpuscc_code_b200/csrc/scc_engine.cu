@@ -182,6 +182,45 @@ struct Eng {
     }
   }
 
+  // The same with two entries per thread, i and i + half (half = ceil(cnt/2)),
+  // so f gets two independent vertices whose dependent loads can overlap.
+  template <class L, class F>
+  __device__ void for_list_pairs_pf(const uint32_t *lst, uint32_t cnt, L &&load, F &&f) {
+    const uint32_t half = (cnt + 1u) / 2u;
+    const uint32_t lim = (half + BS - 1u) / BS * BS;
+    const uint32_t stride = gstride();
+    uint32_t base = blockIdx.x * BS;
+    if (base >= lim) return;
+    auto id = [&](uint32_t i, bool &va, uint32_t &a, bool &vb, uint32_t &b) {
+      va = i < half;
+      vb = i + half < cnt;
+      a = va ? ldm(lst + i) : 0u;
+      b = vb ? ldm(lst + i + half) : 0u;
+    };
+    const uint32_t i0 = base + threadIdx.x;
+    bool a0v, b0v, a1v, b1v;
+    uint32_t a0, b0, a1, b1;
+    id(i0, a0v, a0, b0v, b0);
+    id(i0 + stride, a1v, a1, b1v, b1);
+    auto pa = load(a0, a0v);
+    auto pb = load(b0, b0v);
+    for (; base < lim; base += stride) {
+      bool a2v, b2v;
+      uint32_t a2, b2;
+      id(base + 2u * stride + threadIdx.x, a2v, a2, b2v, b2);
+      auto na = pa, nb = pb;
+      if (base + stride < lim) {
+        na = load(a1, a1v);
+        nb = load(b1, b1v);
+      }
+      f(a0, a0v, pa, b0, b0v, pb);
+      pa = na;
+      pb = nb;
+      a0 = a1, a0v = a1v, b0 = b1, b0v = b1v;
+      a1 = a2, a1v = a2v, b1 = b2, b1v = b2v;
+    }
+  }
+
   template <class L, class F>
   __device__ void for_vertices_pf(L &&load, F &&f) {
     if (list_mode) {
@@ -310,10 +349,8 @@ struct Eng {
     const uint32_t lane = lane_id();
     const bool vec = ((reinterpret_cast<uintptr_t>(g.off) | reinterpret_cast<uintptr_t>(g.offT)) & 15u) == 0;
     const uint32_t step = gstride() * 4u;
-    // stage 1: offsets of four ids (lane 31 also the fifth, which the other
-    // lanes take from their right neighbour)
     struct Quad {
-      uint32_t o[4], t[4], o4, t4;
+      uint32_t o[4], t[4];
     };
     auto load = [&](uint32_t v0) {
       Quad q;
@@ -330,56 +367,43 @@ struct Eng {
           q.t[i] = in ? ldg(g.offT + v0 + i) : 0u;
         }
       }
-      const bool in4 = lane == 31 && v0 + 4u <= n + 1u;
-      q.o4 = in4 ? ldg(g.off + v0 + 4u) : 0u;
-      q.t4 = in4 ? ldg(g.offT + v0 + 4u) : 0u;
       return q;
-    };
-    // stage 2: degree classes, and the heads of single-entry lists (self-
-    // loop test) where the other direction does not already decide
-    struct Heads {
-      uint32_t x[4], y[4];
-      uint32_t code;  // per id i, bits 4i..4i+3: out-degree 0, in-degree 0, out-degree 1, in-degree 1
-    };
-    auto heads = [&](uint32_t v0, const Quad &q) {
-      Heads h;
-      const uint32_t so = __shfl_down_sync(kFull, q.o[0], 1), st = __shfl_down_sync(kFull, q.t[0], 1);
-      const uint32_t o4 = lane == 31 ? q.o4 : so, t4 = lane == 31 ? q.t4 : st;
-      h.code = 0;
-#pragma unroll
-      for (int i = 0; i < 4; ++i) {
-        const uint32_t dout = (i < 3 ? q.o[i + 1] : o4) - q.o[i];
-        const uint32_t din = (i < 3 ? q.t[i + 1] : t4) - q.t[i];
-        const bool valid = v0 + i >= 1u && v0 + i <= n;
-        const bool open = valid && dout != 0 && din != 0;
-        h.x[i] = (open && dout == 1) ? ldg(g.adj + q.o[i]) : 0u;
-        h.y[i] = (open && din == 1) ? ldg(g.adjT + q.t[i]) : 0u;
-        h.code |= ((dout == 0 ? 1u : 0u) | (din == 0 ? 2u : 0u) | (dout == 1 ? 4u : 0u) | (din == 1 ? 8u : 0u))
-                  << (4 * i);
-      }
-      return h;
     };
     uint32_t ntrim = 0;
     uint32_t base = blockIdx.x * BS * 4u;
     const uint32_t wofs = (threadIdx.x >> 5) * 128u + lane * 4u;
     if (base >= lim) return 0;
-    // loads run two iterations ahead, list heads one
-    Quad q1 = load(base + wofs);
-    Heads h0 = heads(base + wofs, q1);
-    if (base + step < lim) q1 = load(base + step + wofs);
+    Quad cur_q = load(base + wofs);
     for (; base < lim; base += step) {
       const uint32_t v0 = base + wofs;
-      Quad q2 = q1;
-      if (base + 2u * step < lim) q2 = load(base + 2u * step + wofs);
-      Heads h1 = h0;
-      if (base + step < lim) h1 = heads(v0 + step, q1);
+      // next iteration's offsets are in flight while this one is decided
+      Quad nxt = cur_q;
+      if (base + step < lim) nxt = load(base + step + wofs);
+      const Quad &q = cur_q;
+      uint32_t o4 = __shfl_down_sync(kFull, q.o[0], 1), t4 = __shfl_down_sync(kFull, q.t[0], 1);
+      if (lane == 31) {
+        const bool in = v0 + 4u <= n + 1u;
+        o4 = in ? ldg(g.off + v0 + 4u) : 0u;
+        t4 = in ? ldg(g.offT + v0 + 4u) : 0u;
+      }
+      // degrees first; the single-entry lists' heads (self-loop test) are
+      // loaded together, and only where the other direction does not decide
+      uint32_t dout[4], din[4], x[4], y[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        dout[i] = (i < 3 ? q.o[i + 1] : o4) - q.o[i];
+        din[i] = (i < 3 ? q.t[i + 1] : t4) - q.t[i];
+        const bool valid = v0 + i >= 1u && v0 + i <= n;
+        const bool open = valid && dout[i] != 0 && din[i] != 0;
+        x[i] = (open && dout[i] == 1) ? ldg(g.adj + q.o[i]) : 0u;
+        y[i] = (open && din[i] == 1) ? ldg(g.adjT + q.t[i]) : 0u;
+      }
       uint32_t bits = 0;
 #pragma unroll
       for (int i = 0; i < 4; ++i) {
         const uint32_t v = v0 + i;
         if (v < 1u || v > n) continue;
-        const uint32_t c = (h0.code >> (4 * i)) & 15u;
-        const bool tr = (c & 3u) != 0 || ((c & 4u) && h0.x[i] == v) || ((c & 8u) && h0.y[i] == v);
+        const bool tr = dout[i] == 0 || din[i] == 0 || (dout[i] == 1 && x[i] == v) || (din[i] == 1 && y[i] == v);
         if (tr) {
           s.label[v] = v;
           bits |= 1u << i;
@@ -397,8 +421,7 @@ struct Eng {
         atomicOr(s.elim + w, word);
         atomicOr(s.tflag + w, word);
       }
-      h0 = h1;
-      q1 = q2;
+      cur_q = nxt;
     }
     return ntrim;
   }
@@ -1062,11 +1085,57 @@ struct Eng {
           stage_put(pq, found, v);
           stage_put(rq, cand && !found, v);
         };
+        // List sweeps take two vertices per thread and probe the aligned 16
+        // bytes holding each list's head together (half of the candidates
+        // find a visited neighbour there); only those that do not go on to
+        // the rest of their list one at a time.
+        const bool vec = (reinterpret_cast<uintptr_t>(padj) & 15u) == 0;
+        auto head = [&](const Pre &p, bool cand, uint4 &q) {
+          const uint32_t a = p.pb & ~3u;
+          const bool h = vec && cand && p.pe > p.pb && (unsigned long long)a + 4ull <= P.g.m;
+          q = h ? __ldg(reinterpret_cast<const uint4 *>(padj + a)) : make_uint4(0u, 0u, 0u, 0u);
+          return h;
+        };
+        auto head_hit = [&](const Pre &p, const uint4 &q, const uint32_t (&w)[4]) {
+          const uint32_t a = p.pb & ~3u;
+          const uint32_t u[4] = {q.x, q.y, q.z, q.w};
+          bool hit = false;
+#pragma unroll
+          for (int j = 0; j < 4; ++j)
+            if (a + j >= p.pb && a + j < p.pe && ((w[j] >> (u[j] & 31u)) & 1u) &&
+                (!ranged || ldm(s.range + u[j]) == p.rv))
+              hit = true;
+          return hit;
+        };
+        auto pair_body = [&](uint32_t va, bool vla, const Pre &pa, uint32_t vb, bool vlb, const Pre &pb) {
+          const bool ca = vla && !(((pa.vw | pa.ew) >> (va & 31u)) & 1u);
+          const bool cb = vlb && !(((pb.vw | pb.ew) >> (vb & 31u)) & 1u);
+          uint4 qa, qb;
+          const bool ha = head(pa, ca, qa), hb = head(pb, cb, qb);
+          uint32_t wa[4], wb[4];
+          const uint32_t ua[4] = {qa.x, qa.y, qa.z, qa.w}, ub[4] = {qb.x, qb.y, qb.z, qb.w};
+#pragma unroll
+          for (int j = 0; j < 4; ++j) {
+            wa[j] = ha ? ldm(vis + (ua[j] >> 5)) : 0u;
+            wb[j] = hb ? ldm(vis + (ub[j] >> 5)) : 0u;
+          }
+          bool fa = ha && head_hit(pa, qa, wa);
+          bool fb = hb && head_hit(pb, qb, wb);
+          if (ca && !fa) fa = any_visited(padj, ha ? (pa.pb & ~3u) + 4u : pa.pb, pa.pe, vis, ranged, pa.rv);
+          if (cb && !fb) fb = any_visited(padj, hb ? (pb.pb & ~3u) + 4u : pb.pb, pb.pe, vis, ranged, pb.rv);
+          if (fa) degsum += pa.pe - pa.pb;
+          if (fb) degsum += pb.pe - pb.pb;
+          warp_set_bits(vis, va, fa, false);
+          warp_set_bits(vis, vb, fb, false);
+          stage_put(pq, fa, va);
+          stage_put(pq, fb, vb);
+          stage_put(rq, ca && !fa, va);
+          stage_put(rq, cb && !fb, vb);
+        };
         if (rem_valid) {
-          for_list_pf(rem_in, rem_n, load, [&](uint32_t v, bool valid, const Pre &p) { body(v, valid, p, false); });
+          for_list_pairs_pf(rem_in, rem_n, load, pair_body);
         } else if (list_mode) {
-          for_list_pf(s.act[act_sel], act_count, load,
-                      [&](uint32_t v, bool valid, const Pre &p) { body(v, valid, p, false); });
+          for_list_pairs_pf(s.act[act_sel], act_count, load, pair_body);
         } else {
           for_vertices_pf(load, [&](uint32_t v, bool valid, const Pre &p) { body(v, valid, p, true); });
         }
