@@ -350,7 +350,7 @@ struct Eng {
     const bool vec = ((reinterpret_cast<uintptr_t>(g.off) | reinterpret_cast<uintptr_t>(g.offT)) & 15u) == 0;
     const uint32_t step = gstride() * 4u;
     struct Quad {
-      uint32_t o[4], t[4], o4, t4;  // o4 / t4: the fifth offsets, loaded by lane 31 only
+      uint32_t o[4], t[4];
     };
     auto load = [&](uint32_t v0) {
       Quad q;
@@ -367,9 +367,6 @@ struct Eng {
           q.t[i] = in ? ldg(g.offT + v0 + i) : 0u;
         }
       }
-      const bool in4 = lane == 31 && v0 + 4u <= n + 1u;
-      q.o4 = in4 ? ldg(g.off + v0 + 4u) : 0u;
-      q.t4 = in4 ? ldg(g.offT + v0 + 4u) : 0u;
       return q;
     };
     uint32_t ntrim = 0;
@@ -384,7 +381,11 @@ struct Eng {
       if (base + step < lim) nxt = load(base + step + wofs);
       const Quad &q = cur_q;
       uint32_t o4 = __shfl_down_sync(kFull, q.o[0], 1), t4 = __shfl_down_sync(kFull, q.t[0], 1);
-      if (lane == 31) o4 = q.o4, t4 = q.t4;
+      if (lane == 31) {
+        const bool in = v0 + 4u <= n + 1u;
+        o4 = in ? ldg(g.off + v0 + 4u) : 0u;
+        t4 = in ? ldg(g.offT + v0 + 4u) : 0u;
+      }
       // degrees first; the single-entry lists' heads (self-loop test) are
       // loaded together, and only where the other direction does not decide
       uint32_t dout[4], din[4], x[4], y[4];
@@ -620,8 +621,6 @@ struct Eng {
         }
       }
       warp_set_bits(s.elim, v, fb, !list_mode);
-      // most sweeps of a large SCC's round eliminate whole warps: no election then
-      if (!__any_sync(kFull, key != kNone)) return;
       const uint32_t grp = __match_any_sync(kFull, key);
       if (key != kNone) {
         const uint32_t hi = (uint32_t)(val >> 32), lo = (uint32_t)val;
