@@ -190,6 +190,36 @@ __device__ __forceinline__ void warp_gather(uint32_t src, uint32_t beg, uint32_t
   }
 }
 
+// warp_gather for visitors that need the whole warp (e.g. warp-staged
+// appends): every lane calls visit(src, dst, tag, valid) at every step, with
+// valid = false (and dst = 0) past the end of the concatenated slices.
+template <class Visit>
+__device__ __forceinline__ void warp_gather_all(uint32_t src, uint32_t beg, uint32_t deg, uint32_t tag,
+                                                const uint32_t *__restrict__ adj, Visit &&visit) {
+  const uint32_t lane = lane_id();
+  const uint32_t incl = warp_incl_scan(deg);
+  const uint32_t total = __shfl_sync(kFull, incl, 31);
+  if (total == 0) return;
+  const uint32_t excl = incl - deg;
+  for (uint32_t b = 0; b < total; b += 32) {
+    const uint32_t e = b + lane;
+    uint32_t lo = 0;
+#pragma unroll
+    for (uint32_t s = 16; s >= 1; s >>= 1) {
+      const uint32_t cand = lo + s;
+      const uint32_t ex = __shfl_sync(kFull, excl, cand & 31u);
+      if (cand < 32 && ex <= e) lo = cand;
+    }
+    const uint32_t o_src = __shfl_sync(kFull, src, lo);
+    const uint32_t o_beg = __shfl_sync(kFull, beg, lo);
+    const uint32_t o_ex = __shfl_sync(kFull, excl, lo);
+    const uint32_t o_tag = __shfl_sync(kFull, tag, lo);
+    const bool valid = e < total;
+    const uint32_t dst = valid ? ldg(adj + o_beg + (e - o_ex)) : 0u;
+    visit(o_src, dst, o_tag, valid);
+  }
+}
+
 // u64 min over a CTA, result valid in thread 0.
 __device__ __forceinline__ unsigned long long block_min_u64(unsigned long long x) {
   __shared__ unsigned long long s_min[32];

@@ -872,6 +872,44 @@ struct Eng {
     P.s.hbase[idx] = (uint32_t)old;
   }
 
+  // heavy_expand for whole-warp visitors: visit(src, dst, tag, valid) on all
+  // lanes at every step (valid = false past the end).
+  template <class Visit>
+  __device__ void heavy_expand_all(const uint32_t *__restrict__ adj, unsigned long long h, Visit &&visit) {
+    const uint32_t cnt = (uint32_t)(h >> 32), tot = (uint32_t)h;
+    if (cnt == 0 || cnt > P.s.hcap) return;  // overflow already flagged by heavy_push
+    const EngState &s = P.s;
+    const uint32_t lane = lane_id();
+    for (uint32_t chunk = gwarp(); (unsigned long long)chunk * 256ull < tot; chunk += nwarps()) {
+      const uint32_t e0 = chunk * 256u;
+      uint32_t j = 0;
+      if (lane == 0) {  // largest j with hbase[j] <= e0
+        uint32_t lo = 0, hi = cnt - 1;
+        while (lo < hi) {
+          const uint32_t mid = (lo + hi + 1) >> 1;
+          if (ldm(s.hbase + mid) <= e0) lo = mid;
+          else hi = mid - 1;
+        }
+        j = lo;
+      }
+      j = __shfl_sync(kFull, j, 0);
+      for (uint32_t sft = 0; sft < 256u; sft += 32u) {
+        if (e0 + sft >= tot) break;
+        const uint32_t e = e0 + sft + lane;
+        const bool valid = e < tot;
+        uint32_t src = 0, dst = 0, tag = 0;
+        if (valid) {
+          uint32_t jj = j;
+          while (jj + 1 < cnt && ldm(s.hbase + jj + 1) <= e) ++jj;
+          dst = ldg(adj + ldm(s.hbeg + jj) + (e - ldm(s.hbase + jj)));
+          src = ldm(s.hv + jj);
+          tag = ldm(s.htag + jj);
+        }
+        visit(src, dst, tag, valid);
+      }
+    }
+  }
+
   template <class Visit>
   __device__ void heavy_expand(const uint32_t *__restrict__ adj, unsigned long long h, Visit &&visit) {
     const uint32_t cnt = (uint32_t)(h >> 32), tot = (uint32_t)h;
@@ -1156,6 +1194,17 @@ struct Eng {
         const unsigned long long per_warp = mf / nwarps();
         uint32_t split = heavy;
         if (allow_pull && per_warp < heavy) split = per_warp < 256ull ? 256u : (uint32_t)per_warp;
+        // newly reached vertices go to the next frontier through warp-staged
+        // appends (one global atomic per 224 items, not per coalesced group)
+        auto claim = [&](uint32_t u, uint32_t rsrc, bool valid) {
+          const bool claimed = valid && try_visit(vis, u, ranged, rsrc);
+          if (claimed && allow_pull) degsum += ldg(off + u + 1) - ldg(off + u);
+          return claimed;
+        };
+        Stage fq{out, cnt, s.qcap, 0, stage_buf()};
+        auto visit_all = [&](uint32_t, uint32_t u, uint32_t rsrc, bool valid) {
+          stage_put(fq, claim(u, rsrc, valid), u);
+        };
         for_items(nin, [&](uint32_t i, bool valid) {
           uint32_t v = 0, b = 0, d = 0, rv = 0;
           if (valid) {
@@ -1168,8 +1217,9 @@ struct Eng {
               d = 0;
             }
           }
-          warp_gather(v, b, d, rv, adj, visit);
+          warp_gather_all(v, b, d, rv, adj, visit_all);
         });
+        stage_flush(fq);
         add_count(cur() + C_DEG, degsum);
         if (!bar(700)) return depth;
         const unsigned long long h = ldm64(prv64());
@@ -1179,7 +1229,11 @@ struct Eng {
           cnt = cur() + C_Q;
           if (is_lead()) atomicAdd(cur() + C_DEG, rdprv(C_DEG));
           degsum = 0;
-          heavy_expand(adj, h, visit);
+          Stage hq{out + qoff, cnt, s.qcap - qoff, 0, stage_buf()};
+          heavy_expand_all(adj, h, [&](uint32_t, uint32_t u, uint32_t rsrc, bool valid) {
+            stage_put(hq, claim(u, rsrc, valid), u);
+          });
+          stage_flush(hq);
           add_count(cur() + C_DEG, degsum);
           if (!bar(701)) return depth;
           prof(PR_HEAVY, th, (uint32_t)(h >> 32), (uint32_t)h);
