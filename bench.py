@@ -240,7 +240,7 @@ def run_ours(args) -> None:
         import datetime
 
         import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     import gpuscc_code_b200 as scc
 
     scale, samples = args.scale, 1 << args.samples_log2
