@@ -599,7 +599,11 @@ struct Eng {
       const uint32_t w = v >> 5;
       return Pre{ldm(s.elim + w), ldm(s.fvis + w), ldm(s.bvis + w), ldm(s.range + (valid ? v : 0u))};
     };
-    // A: eliminate F∩B, elect pivots (CTA-local min per key, flushed below)
+    // A: eliminate F∩B, elect pivots (CTA-local min per key, flushed below).
+    // A partition id is its pivot's id (rpivot[r] == r) once pivots have been
+    // elected; only the first round of a single partition still runs under
+    // id 0, whose pivot is rpivot[0] -- so no per-vertex rpivot load.
+    const uint32_t p0 = ldm(s.rpivot);
     for_vertices_pf(load, [&](uint32_t v, bool valid, const Pre &pre) {
       const uint32_t ew = pre.ew, fw = pre.fw, bw = pre.bw;
       if (!list_mode && ~ew == 0u) return;  // whole word already eliminated
@@ -610,7 +614,7 @@ struct Eng {
       if (valid && !((ew >> (v & 31u)) & 1u)) {
         const bool f = (fw >> (v & 31u)) & 1u, b = (bw >> (v & 31u)) & 1u;
         if (f && b) {
-          const uint32_t p = ldm(s.rpivot + r);
+          const uint32_t p = r ? r : p0;
           s.label[v] = p;
           fb = true;
           ++nelim;
