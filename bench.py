@@ -656,8 +656,33 @@ def run_refgpu(args) -> None:
                 ref["count_matches"] = ref["nscc"] == cnt
                 ref["speedup_of_ours"] = ref["secs"] / row["ours_h"]["secs"]
         rows.append(row)
+    # the mixed batch: the reference solves graphs one at a time (a sample of
+    # them), the engine all 4096 in one captured launch
+    batch = {"graphs": 4096, "reference_sample": args.refgpu_batch}
+    try:
+        r = subprocess.run([sys.executable, "-m", "oracle.ref_gpu", "--batch", str(args.refgpu_batch), "--alg", "h"],
+                           cwd=ROOT, capture_output=True, text=True, timeout=args.refgpu_timeout)
+        batch["reference_h"] = json.loads(r.stdout.strip().splitlines()[-1]) if r.returncode == 0 else {
+            "error": f"exit {r.returncode}: {(r.stderr or r.stdout).strip()[-200:]}"}
+    except subprocess.TimeoutExpired:
+        batch["reference_h"] = {"error": f"no result within {args.refgpu_timeout} s"}
+    ctx = scc.SCCContext(0, scc.Options(alg="h", wcc=True, trim2=True))
+    ctx.gen_batch_device(4096, 1000, 200_000, 2.0, 16.0, seed=4)
+    ctx.capture()
+    for _ in range(3):
+        ctx.replay()
+    ms = []
+    for _ in range(5):
+        _, st = ctx.replay()
+        ms.append(st["ms_total"])
+    ctx.close()
+    batch["ours_batched_graphs_per_s"] = 4096 / (statistics.median(ms) / 1e3)
+    ref = batch["reference_h"]
+    if "graphs_per_s_timer" in ref:
+        batch["speedup_vs_reference_timer"] = batch["ours_batched_graphs_per_s"] / ref["graphs_per_s_timer"]
+        batch["speedup_vs_reference_wall"] = batch["ours_batched_graphs_per_s"] / ref["graphs_per_s_wall"]
     print(json.dumps({"metric": "SCC solve time vs the reference's GPU FB (same B200, same graphs)",
-                      "unit": "s", "rows": rows,
+                      "unit": "s", "rows": rows, "batch": batch,
                       "note": "reference: scc.cu computeSCC of the scc_2_w build (-DWCC -DTRIM_2), its own timer; "
                               "ours: scc_2_w -a h, CUDA events, median of 5"}), flush=True)
 
@@ -685,6 +710,7 @@ def main():
     ap.add_argument("--refgpu-grid", type=int, default=1024, help="refgpu: grid side")
     ap.add_argument("--refgpu-algs", nargs="*", default=["h", "t"], help="refgpu: reference -a arms")
     ap.add_argument("--refgpu-timeout", type=int, default=300)
+    ap.add_argument("--refgpu-batch", type=int, default=256, help="refgpu: batch graphs the reference solves")
     ap.add_argument("--workload", choices=["rmat26", "grid", "batch", "serve", "refgpu"], default="rmat26",
                     help="rmat26: the headline line; batch: 4096 packed graphs in one launch vs one launch each; "
                          "serve: Poisson stream through the request loop (plain / batched / batched + network); "

@@ -64,9 +64,37 @@ def main():
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--alg", default="h", choices=list(ALGS))
     ap.add_argument("--repeats", type=int, default=2)
+    ap.add_argument("--batch", type=int, default=0,
+                    help="solve the first N graphs of the 4096-graph batch (ER / R-MAT, n in [1e3, 2e5], "
+                         "degree 2-16, seed 4) one by one")
     args = ap.parse_args()
     sys.path.insert(0, str(HERE.parent))
     import gpuscc_code_b200 as scc
+    if args.batch:
+        import numpy as np
+        with scc.SCCContext(0) as ctx:
+            seg = ctx.gen_batch_device(4096, 1000, 200_000, 2.0, 16.0, seed=4)
+            full = ctx.download()
+        nodes, edges, nodesT, edgesT = (np.asarray(a) for a in (full.nodes, full.edges, full.nodesT, full.edgesT))
+        tot_secs = tot_wall = 0.0
+        tot_cnt = 0
+        for gi in range(args.batch):
+            lo, hi = int(seg[gi]), int(seg[gi + 1])
+            e0, e1, t0, t1 = int(nodes[lo]), int(nodes[hi]), int(nodesT[lo]), int(nodesT[hi])
+            k = hi - lo
+            ln = np.zeros(k + 2, np.uint32)
+            ln[1:] = nodes[lo:hi + 1] - e0
+            lt = np.zeros(k + 2, np.uint32)
+            lt[1:] = nodesT[lo:hi + 1] - t0
+            g = scc.HostCSR.from_arrays(ln, edges[e0:e1] - (lo - 1), lt, edgesT[t0:t1] - (lo - 1), sorted_unique=True)
+            cnt, secs, wall = run(g, args.alg)
+            tot_secs += secs
+            tot_wall += wall
+            tot_cnt += cnt
+        print(json.dumps({"graphs": args.batch, "nscc_total": tot_cnt, "alg": args.alg, "secs": tot_secs,
+                          "wall_s": tot_wall, "graphs_per_s_timer": args.batch / tot_secs,
+                          "graphs_per_s_wall": args.batch / tot_wall}), flush=True)
+        return
     if args.grid:
         g = scc.gen_grid(args.grid, 0.15, 0.001, seed=args.seed)
     else:
