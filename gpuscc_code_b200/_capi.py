@@ -147,6 +147,8 @@ SIGNATURES = [
     ("scc_get_states", C.c_int, [C.c_void_p, C.POINTER(C.c_uint8)]),
     ("scc_get_ranges", C.c_int, [C.c_void_p, u32p]),
     ("scc_get_labels", C.c_int, [C.c_void_p, u32p, u32p]),
+    ("scc_batch_pack", C.c_int, [C.c_uint32, C.POINTER(scc_host_csr), C.POINTER(scc_host_csr), u32p]),
+    ("scc_batch_solve", C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(scc_host_csr), C.POINTER(u32p), u32p]),
     ("scc_graph_features", C.c_int, [C.c_void_p, f32p]),
     ("scc_mlp_create", C.c_int, [C.c_int, C.c_uint64, C.POINTER(C.c_void_p)]),
     ("scc_mlp_destroy", C.c_int, [C.c_void_p]),

@@ -745,6 +745,38 @@ int scc_solve(scc_ctx *c, uint32_t *labels, uint32_t *nscc, scc_stats *st) {
   return SCC_OK;
 }
 
+int scc_batch_solve(scc_ctx *c, uint32_t count, const scc_host_csr *graphs, uint32_t *const *labels,
+                    uint32_t *nscc) {
+  sccb::clear_error();
+  if (!c || (count && !graphs)) return set_error(SCC_ERR_INVALID, "null argument");
+  if (count == 0) return SCC_OK;
+  std::vector<uint32_t> seg(count + 1);
+  scc_host_csr packed;
+  int rc = scc_batch_pack(count, graphs, &packed, seg.data());
+  if (rc) return rc;
+  std::vector<uint32_t> all((size_t)packed.n + 1);
+  rc = scc_ctx_upload(c, &packed);
+  if (!rc) rc = scc_ctx_set_segments(c, count, seg.data());
+  uint32_t total = 0;
+  if (!rc) rc = scc_solve(c, all.data(), &total, nullptr);
+  scc_ctx_set_segments(c, 0, nullptr);
+  scc_host_csr_free(&packed);
+  if (rc) return rc;
+  // global ids -> each graph's own ids; a component's label is its smallest id
+  for (uint32_t g = 0; g < count; ++g) {
+    const uint32_t base = seg[g] - 1, n = graphs[g].n;
+    uint32_t roots = 0;
+    for (uint32_t v = 1; v <= n; ++v) {
+      const uint32_t l = all[base + v] - base;
+      roots += l == v;
+      if (labels && labels[g]) labels[g][v] = l;
+    }
+    if (labels && labels[g]) labels[g][0] = 0;
+    if (nscc) nscc[g] = roots;
+  }
+  return SCC_OK;
+}
+
 int scc_get_profile(scc_ctx *c, double *ms, uint32_t *counts) {
   sccb::clear_error();
   if (!c) return set_error(SCC_ERR_INVALID, "null context");

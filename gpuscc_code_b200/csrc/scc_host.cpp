@@ -176,6 +176,58 @@ void scc_host_csr_free(scc_host_csr *c) {
   std::memset(c, 0, sizeof(*c));
 }
 
+int scc_batch_pack(uint32_t count, const scc_host_csr *graphs, scc_host_csr *out, uint32_t *seg_first) {
+  sccb::clear_error();
+  if (!out || !seg_first || (count && !graphs)) return set_error(SCC_ERR_INVALID, "null argument");
+  uint64_t N = 0, M = 0;
+  bool sorted = true;
+  for (uint32_t g = 0; g < count; ++g) {
+    const scc_host_csr &c = graphs[g];
+    if (!c.nodes || !c.nodesT || (c.m && (!c.edges || !c.edgesT)))
+      return set_error(SCC_ERR_INVALID, "graph %u: arrays missing", g);
+    if (c.nodes[c.n + 1] != c.m || c.nodesT[c.n + 1] != c.m)
+      return set_error(SCC_ERR_INVALID, "graph %u: offsets end at %u/%u, expected m = %u", g, c.nodes[c.n + 1],
+                       c.nodesT[c.n + 1], c.m);
+    N += c.n;
+    M += c.m;
+    sorted = sorted && c.sorted_unique;
+  }
+  if (N >= (1ull << 30) || M >= (1ull << 32)) return set_error(SCC_ERR_CAPACITY, "packed batch exceeds 32-bit ids");
+  std::vector<uint32_t> off(N + 2), offT(N + 2), adj(M + 1), adjT(M + 1);
+  uint32_t vb = 0, eb = 0;
+  seg_first[0] = 1;
+  for (uint32_t g = 0; g < count; ++g) {
+    const scc_host_csr &c = graphs[g];
+    for (uint32_t v = 1; v <= c.n + 1; ++v) {  // entry n+1 equals the next graph's first
+      off[vb + v] = c.nodes[v] + eb;
+      offT[vb + v] = c.nodesT[v] + eb;
+    }
+    for (uint32_t j = 0; j < c.m; ++j) {
+      adj[eb + j] = c.edges[j] + vb;
+      adjT[eb + j] = c.edgesT[j] + vb;
+    }
+    vb += c.n;
+    eb += c.m;
+    seg_first[g + 1] = vb + 1;
+  }
+  off[N + 1] = offT[N + 1] = (uint32_t)M;
+  std::memset(out, 0, sizeof(*out));
+  out->n = (uint32_t)N;
+  out->m = (uint32_t)M;
+  out->nnz_header = (uint32_t)M;
+  out->sorted_unique = sorted ? 1 : 0;
+  out->owned = 1;
+  out->nodes = dup_array(off, 0);
+  out->edges = dup_array(adj, 0);
+  out->nodesT = dup_array(offT, 0);
+  out->edgesT = dup_array(adjT, 0);
+  if (!out->nodes || !out->edges || !out->nodesT || !out->edgesT) {
+    scc_host_csr_free(out);
+    return set_error(SCC_ERR_NOMEM, "host allocation of the packed batch failed");
+  }
+  return SCC_OK;
+}
+
 int scc_csr_from_edges(uint32_t n, uint64_t n_edges, const uint32_t *src, const uint32_t *dst, int drop_self_loops,
                        scc_host_csr *out) {
   sccb::clear_error();

@@ -133,7 +133,6 @@ struct scc_server {
   bool stopping = false;
   scc_server_stats st{};
   std::thread admit_thr, solve_thr;
-  int fatal = SCC_OK;
 
   void admit_loop();
   void solve_loop();

@@ -231,6 +231,17 @@ int scc_solve_device(scc_ctx *ctx, uint32_t *d_labels, uint32_t *nscc, scc_stats
  * result like scc_solve_collect.  Re-capture after binding another graph. */
 int scc_solve_capture(scc_ctx *ctx, uint32_t *d_labels);
 int scc_solve_replay(scc_ctx *ctx, uint32_t *nscc, scc_stats *stats);
+/* Batching (no counterpart in the reference, which solves one graph per run).
+ * scc_batch_pack: independent graphs (reference layout each) into one CSR
+ * with disjoint id ranges -- graph g owns ids seg_first[g] .. seg_first[g+1]-1
+ * (seg_first: count+1 entries); out is owned by the library
+ * (scc_host_csr_free).  scc_batch_solve: pack, upload, solve all graphs in
+ * one persistent launch with one partition per graph, and return each
+ * graph's labels in its own ids (labels[g]: host n_g+1, or NULL) and SCC
+ * count (nscc[g], or NULL). */
+int scc_batch_pack(uint32_t count, const scc_host_csr *graphs, scc_host_csr *out, uint32_t *seg_first);
+int scc_batch_solve(scc_ctx *ctx, uint32_t count, const scc_host_csr *graphs, uint32_t *const *labels,
+                    uint32_t *nscc);
 /* Copy the labels of the last solve that wrote the context's own label
  * buffer (d_labels = NULL) to the host: labels (n+1). */
 int scc_read_labels(scc_ctx *ctx, uint32_t *labels);

@@ -62,3 +62,26 @@ def test_all_arms_in_one_run():
     r = run("scc_2_w", "-a", "a", "-f", str(GOLDEN / "demo.graph"))
     assert r.returncode == 0, r.stderr
     assert counts(r.stdout) == [6] * 7
+
+
+@pytest.mark.gpu
+def test_verify_files_follow_the_labels(tmp_path):
+    golden = json.load(open(GOLDEN / "golden.json"))
+    for name in ("demo.graph", "cycles.graph", "general.mtx"):
+        labels = golden[name]["labels"]
+        d = tmp_path / name.replace(".", "_")
+        d.mkdir()
+        r = run("scc_2_w", "-a", "h", "-f", str(GOLDEN / name), "-v", str(d))
+        assert r.returncode == 0, r.stderr
+        groups = {}
+        for v in range(1, len(labels)):
+            groups.setdefault(labels[v], []).append(v)
+        sccs = [list(map(int, l.split())) for l in (d / "parallel_scc.txt").read_text().splitlines()]
+        assert sccs == [groups[k] for k in sorted(groups)]
+        trivial = [int(l) for l in (d / "trivial.txt").read_text().splitlines()]
+        assert trivial == sorted(k for k, m in groups.items() if len(m) == 1)
+        dist = dict(tuple(map(int, l.split())) for l in (d / "scc_dist.txt").read_text().splitlines())
+        sizes = {}
+        for m in groups.values():
+            sizes[len(m)] = sizes.get(len(m), 0) + 1
+        assert dist == sizes
