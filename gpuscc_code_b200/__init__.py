@@ -6,6 +6,6 @@ Python host binding.  Importing it fails if the library is not built.
 """
 from ._capi import ALG, SCCError, lib  # noqa: F401  (raises ImportError when the .so is missing)
 from .scc import (HostCSR, Options, SCCContext, computeSCC, csr_from_edges, gen_batch, gen_er, gen_grid,  # noqa: F401
-                  gen_rmat, load, tarjan)
+                  gen_rmat, load, save, tarjan)
 
 __version__ = lib.scc_version().decode()

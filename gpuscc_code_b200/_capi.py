@@ -102,6 +102,7 @@ SIGNATURES = [
     ("scc_opts_default", None, [C.POINTER(scc_opts)]),
     ("scc_load", C.c_int, [C.c_char_p, C.c_int, C.POINTER(scc_host_csr)]),
     ("scc_host_csr_free", None, [C.POINTER(scc_host_csr)]),
+    ("scc_save", C.c_int, [C.c_char_p, C.POINTER(scc_host_csr)]),
     ("scc_csr_from_edges", C.c_int, [C.c_uint32, C.c_uint64, u32p, u32p, C.c_int, C.POINTER(scc_host_csr)]),
     ("scc_tarjan", C.c_int, [C.POINTER(scc_host_csr), u32p, u32p, C.POINTER(C.c_double)]),
     ("scc_gen_rmat", C.c_int, [C.c_uint32, C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint64, C.c_int,

@@ -80,6 +80,138 @@ uint32_t *dup_array(const std::vector<uint32_t> &v, size_t extra) {
   return p;
 }
 
+// ------------------------------------------------------------ loader helpers
+constexpr char kBinMagic[8] = {'S', 'C', 'C', 'B', 'C', 'S', 'R', '1'};
+// edge sections at least this long are parsed by all host threads
+constexpr size_t kParallelParseBytes = 8u << 20;
+
+struct BinHeader {
+  char magic[8];
+  uint32_t n, m, nnz_header;
+  int32_t symmetric, sorted_unique, pad;
+};
+
+// Edge lines of a text graph split into one chunk per thread at line
+// boundaries; each chunk is parsed on its own, then the first nnz non-blank
+// lines are kept in file order, exactly as the serial reader would take them
+// (a malformed line after those is never looked at, as in load.cpp).
+int parse_edges_parallel(const char *path, const char *p, const char *end, uint32_t n, long long nnz,
+                         bool symmetric, std::vector<uint32_t> &src, std::vector<uint32_t> &dst,
+                         long long &count_edges) {
+  const unsigned nt = hw_threads();
+  std::vector<const char *> cut(nt + 1);
+  cut[0] = p;
+  cut[nt] = end;
+  for (unsigned t = 1; t < nt; ++t) {
+    const char *c = p + (size_t)(end - p) * t / nt;
+    if (c < cut[t - 1]) c = cut[t - 1];
+    while (c < end && c[-1] != '\n') ++c;
+    cut[t] = c;
+  }
+  struct Part {
+    std::vector<uint32_t> d, s;  // one entry per line (symmetric copies added later)
+    long long bad_line = -1;     // first malformed or out-of-range line in this chunk
+    int bad_kind = 0;            // 1 = unparsable, 2 = vertex out of range
+  };
+  std::vector<Part> parts(nt);
+  std::vector<std::thread> th;
+  for (unsigned t = 0; t < nt; ++t) {
+    th.emplace_back([&, t] {
+      Part &pt = parts[t];
+      const char *q = cut[t], *qe = cut[t + 1];
+      auto skip_ws = [&] {
+        while (q < qe && (*q == ' ' || *q == '\t' || *q == '\r')) ++q;
+      };
+      auto read_int = [&](long long &x) -> bool {
+        skip_ws();
+        bool neg = false;
+        if (q < qe && (*q == '-' || *q == '+')) neg = *q++ == '-';
+        if (q >= qe || *q < '0' || *q > '9') return false;
+        long long v = 0;
+        while (q < qe && *q >= '0' && *q <= '9') v = v * 10 + (*q++ - '0');
+        x = neg ? -v : v;
+        return true;
+      };
+      while (q < qe) {
+        skip_ws();
+        if (q < qe && *q == '\n') {
+          ++q;
+          continue;
+        }
+        if (q >= qe) break;
+        long long d = 0, sv = 0;
+        const bool ok = read_int(d) && read_int(sv);
+        while (q < qe && *q != '\n') ++q;
+        if (q < qe) ++q;
+        if (pt.bad_line < 0 && (!ok || d < 1 || d > n || sv < 1 || sv > n)) {
+          pt.bad_line = (long long)pt.d.size();
+          pt.bad_kind = ok ? 2 : 1;
+        }
+        pt.d.push_back(ok ? (uint32_t)d : 0u);
+        pt.s.push_back(ok ? (uint32_t)sv : 0u);
+      }
+    });
+  }
+  for (auto &x : th) x.join();
+  long long seen = 0;
+  for (unsigned t = 0; t < nt && seen < nnz; ++t) {
+    const Part &pt = parts[t];
+    const long long take = std::min<long long>((long long)pt.d.size(), nnz - seen);
+    if (pt.bad_line >= 0 && pt.bad_line < take) {
+      const long long line = seen + pt.bad_line + 1;
+      if (pt.bad_kind == 1) return sccb::set_error(SCC_ERR_IO, "%s: bad edge line %lld", path, line);
+      return sccb::set_error(SCC_ERR_IO, "%s: edge line %lld names a vertex outside 1..%u", path, line, n);
+    }
+    for (long long i = 0; i < take; ++i) {
+      const uint32_t d = pt.d[i], sv = pt.s[i];
+      src.push_back(sv);  // edge src -> dst (load.cpp:78-93)
+      dst.push_back(d);
+      if (symmetric && d != sv) {
+        src.push_back(d);
+        dst.push_back(sv);
+        ++count_edges;
+      }
+    }
+    seen += take;
+  }
+  if (seen < nnz) return sccb::set_error(SCC_ERR_IO, "%s: %lld edge lines expected, %lld found", path, nnz, seen);
+  return SCC_OK;
+}
+
+int load_binary(const char *path, const std::string &buf, scc_host_csr *out) {
+  BinHeader h;
+  if (buf.size() < sizeof(h)) return sccb::set_error(SCC_ERR_IO, "%s: truncated binary CSR", path);
+  std::memcpy(&h, buf.data(), sizeof(h));
+  const uint64_t words = 2ull * (h.n + 2ull) + 2ull * h.m;
+  if (h.n >= (1u << 30) || buf.size() != sizeof(h) + words * 4)
+    return sccb::set_error(SCC_ERR_IO, "%s: binary CSR size does not match its header", path);
+  const uint32_t *w = reinterpret_cast<const uint32_t *>(buf.data() + sizeof(h));
+  std::vector<uint32_t> off(w, w + h.n + 2), adj(w + h.n + 2, w + h.n + 2 + h.m);
+  std::vector<uint32_t> offT(w + h.n + 2 + h.m, w + 2 * (h.n + 2) + h.m), adjT(w + 2 * (h.n + 2) + h.m, w + words);
+  if (off[h.n + 1] != h.m || offT[h.n + 1] != h.m) return sccb::set_error(SCC_ERR_IO, "%s: binary CSR offsets corrupt", path);
+  std::memset(out, 0, sizeof(*out));
+  out->n = h.n;
+  out->m = h.m;
+  out->nnz_header = h.nnz_header;
+  out->sorted_unique = h.sorted_unique;
+  out->owned = 1;
+  out->nodes = dup_array(off, 0);
+  out->edges = dup_array(adj, 1);
+  if (h.symmetric) {
+    out->nodesT = out->nodes;
+    out->edgesT = out->edges;
+    out->symmetric = 1;
+  } else {
+    out->nodesT = dup_array(offT, 0);
+    out->edgesT = dup_array(adjT, 1);
+  }
+  if (!out->nodes || !out->edges || !out->nodesT || !out->edgesT) {
+    scc_host_csr_free(out);
+    return sccb::set_error(SCC_ERR_NOMEM, "host allocation of %u-vertex CSR failed", h.n);
+  }
+  return SCC_OK;
+}
+
 }  // namespace
 
 namespace sccb {
@@ -238,6 +370,28 @@ int scc_csr_from_edges(uint32_t n, uint64_t n_edges, const uint32_t *src, const 
 
 // ---------------------------------------------------------------- loader
 // load.cpp:18-207, same semantics, linear-time parsing.
+int scc_save(const char *path, const scc_host_csr *g) {
+  sccb::clear_error();
+  if (!path || !g || !g->nodes || !g->nodesT || (g->m && (!g->edges || !g->edgesT)))
+    return set_error(SCC_ERR_INVALID, "null argument");
+  FILE *f = std::fopen(path, "wb");
+  if (!f) return set_error(SCC_ERR_IO, "cannot create %s", path);
+  BinHeader h{};
+  std::memcpy(h.magic, kBinMagic, 8);
+  h.n = g->n;
+  h.m = g->m;
+  h.nnz_header = g->nnz_header;
+  h.symmetric = g->symmetric;
+  h.sorted_unique = g->sorted_unique;
+  bool ok = std::fwrite(&h, sizeof(h), 1, f) == 1;
+  ok = ok && std::fwrite(g->nodes, 4, (size_t)g->n + 2, f) == (size_t)g->n + 2;
+  ok = ok && std::fwrite(g->edges, 4, g->m, f) == g->m;
+  ok = ok && std::fwrite(g->nodesT, 4, (size_t)g->n + 2, f) == (size_t)g->n + 2;
+  ok = ok && std::fwrite(g->edgesT, 4, g->m, f) == g->m;
+  ok = std::fclose(f) == 0 && ok;
+  return ok ? SCC_OK : set_error(SCC_ERR_IO, "writing %s failed", path);
+}
+
 int scc_load(const char *path, int header, scc_host_csr *out) {
   (void)header;  // load.cpp ignores it as well
   sccb::clear_error();
@@ -262,6 +416,7 @@ int scc_load(const char *path, int header, scc_host_csr *out) {
     pos = e + 1;
     return true;
   };
+  if (buf.size() >= 8 && std::memcmp(buf.data(), kBinMagic, 8) == 0) return load_binary(path, buf, out);
   std::string line;
   if (!next_line(line)) return set_error(SCC_ERR_IO, "%s: empty file", path);
   const bool pattern = std::strstr(line.c_str(), "pattern") != nullptr;
@@ -301,6 +456,10 @@ int scc_load(const char *path, int header, scc_host_csr *out) {
     x = neg ? -v : v;
     return true;
   };
+  if ((size_t)(end - p) >= kParallelParseBytes && hw_threads() > 1) {
+    int prc = parse_edges_parallel(path, p, end, n, nnz, symmetric, src, dst, count_edges);
+    if (prc != SCC_OK) return prc;
+  } else
   for (long long i = 0; i < nnz;) {
     // skip blank lines
     skip_ws();

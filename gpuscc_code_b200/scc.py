@@ -20,7 +20,7 @@ import numpy as np
 from ._capi import (ALG, SCCError, check, lib, scc_dev_csr, scc_host_csr, scc_opts, scc_stats, u32p)
 
 __all__ = [
-    "HostCSR", "load", "csr_from_edges", "gen_rmat", "gen_er", "gen_grid", "tarjan", "Options",
+    "HostCSR", "load", "save", "csr_from_edges", "gen_rmat", "gen_er", "gen_grid", "tarjan", "Options",
     "SCCContext", "computeSCC", "SCCError",
 ]
 
@@ -105,6 +105,11 @@ def load(path: str, header: bool = False) -> HostCSR:
     raw = scc_host_csr()
     check(lib.scc_load(str(path).encode(), int(header), C.byref(raw)))
     return HostCSR(raw)
+
+
+def save(g: HostCSR, path: str) -> None:
+    """Binary CSR cache: load() reads it back without parsing."""
+    check(lib.scc_save(str(path).encode(), C.byref(g.raw)))
 
 
 def csr_from_edges(n: int, src, dst, drop_self_loops: bool = False) -> HostCSR:

@@ -116,6 +116,12 @@ typedef struct scc_host_csr {
  * std::set.  Returns SCC_ERR_IO instead of exit(1). */
 int scc_load(const char *path, int header, scc_host_csr *out);
 void scc_host_csr_free(scc_host_csr *csr);
+/* Binary CSR cache (no counterpart in the reference, whose text parse
+ * dominates its run time on large graphs): scc_save writes the CSR and
+ * transpose as they are; scc_load recognises such a file by its first bytes
+ * and reads it without parsing.  Large text files are parsed by all host
+ * threads (same result as the serial reader, load.cpp semantics). */
+int scc_save(const char *path, const scc_host_csr *csr);
 /* Build a host CSR (+transpose) from an edge list of 1-based (src, dst) pairs:
  * duplicates merged, lists sorted, self-loops kept unless drop_self_loops. */
 int scc_csr_from_edges(uint32_t n, uint64_t n_edges, const uint32_t *src, const uint32_t *dst,
