@@ -445,6 +445,8 @@ def run_batch(args) -> None:
         ev1.synchronize()
         ms_dev.append(ev0.elapsed_time(ev1))
     batched_ms = statistics.median(ms_dev)
+    batch_profile = ctx.profile()  # device phase timers of the last replay
+    batch_stats = st
     # the same graphs, one launch each (local ids, uploaded and solved one by one)
     full = ctx.download()
     nodes, edges, nodesT, edgesT = (np.asarray(a) for a in (full.nodes, full.edges, full.nodesT, full.edgesT))
@@ -492,6 +494,8 @@ def run_batch(args) -> None:
         "speedup_vs_per_graph": {"wall": (count / (batched_ms / 1e3)) / (count / wall),
                                  "device": dev_sum / batched_ms},
         "gpu_launches": 2,
+        "profile_ms": batch_profile,
+        "stats": {k: (round(v, 4) if isinstance(v, float) else v) for k, v in batch_stats.items()},
     }
     print(json.dumps(line), flush=True)
     per.close()

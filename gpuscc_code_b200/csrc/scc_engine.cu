@@ -1603,7 +1603,10 @@ struct Eng {
       }
       const uint32_t nel = ldm(&c->n_fbe) + ldm(&c->n_trim2);
       const uint32_t arm = arm_for(nel < o.switch_thr);
-      const bool ranged = !(step == 1 && single);
+      // In the first round every partition is a whole segment (one graph of a
+      // batch, or the graph) and no edge leaves a segment, so the reach and
+      // trim of that round need no partition test.
+      const bool ranged = step != 1;
       t0 = globaltimer_ns();
       const uint32_t fd = reach(0, arm, ranged);
       timed(c->ns_fwd, t0);
