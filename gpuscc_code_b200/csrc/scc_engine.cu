@@ -1483,11 +1483,11 @@ struct Eng {
     refresh_mode();
   }
 
-  // compacts when fewer than span / ratio vertices are live
-  __device__ void maybe_compact(uint32_t ratio = 4) {
+  // compacts when fewer than span * den / num vertices are live
+  __device__ void maybe_compact(uint32_t num = 4, uint32_t den = 1) {
     const uint32_t nlive = ldm(&c->n_live);
     const uint32_t span = list_mode ? act_count : P.g.n;
-    if (nlive > 0 && (unsigned long long)nlive * ratio < span) compact();
+    if (nlive > 0 && (unsigned long long)nlive * num < (unsigned long long)span * den) compact();
   }
 
   __device__ void sync_live() {
@@ -1575,7 +1575,7 @@ struct Eng {
       // power-law graphs lose most vertices to the first trim: sweep the
       // survivors' list from the first round on
       const unsigned long long tc = globaltimer_ns();
-      maybe_compact(2);
+      maybe_compact(5, 4);
       prof(PR_COMPACT, tc);
     }
     timed(c->ns_trim, t0);
