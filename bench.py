@@ -1,27 +1,37 @@
 #!/usr/bin/env python
 """SCC throughput on B200: edges/s and HBM-roofline fraction of the scc_2_w path.
 
-Workload (one step = one complete decomposition): R-MAT, 2^26 vertices,
-2^30 edge samples, (a,b,c,d) = (0.57, 0.19, 0.19, 0.05), vertex ids permuted,
-self-loops dropped, duplicates merged, seed 2, u32 CSR + transpose resident in
-HBM; path = scc_2_w -a h (global trim-1, hybrid reach, WCC colouring and
-trim-2 once, then partition rounds), labels written to device memory.
+Headline workload (one step = one complete decomposition): R-MAT, 2^26
+vertices, 2^30 edge samples, (a,b,c,d) = (0.57, 0.19, 0.19, 0.05), vertex ids
+permuted, self-loops dropped, duplicates merged, seed 2, u32 CSR + transpose
+resident in HBM; path = scc_2_w -a h (global trim-1, hybrid reach, WCC
+colouring and trim-2 once, then partition rounds), labels written to device
+memory.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-value   = m / device time per step (CUDA events on the engine's stream), summed
-          over replicas for N > 1 (a single graph does not shard: N independent
-          replicas, no collective; scaling "weak").
-e2e     = the same metric through the public API from pinned host buffers:
-          each step uploads the CSR (+ device validation), solves and copies
-          the labels back.
-roofline: bytes the decomposition must touch, 2*4(n+1) + 2*4m + 4n (offsets
-          and adjacency of the graph and its transpose once, one u32 label per
-          vertex), divided by the step's device time, against the measured HBM
-          copy bandwidth in MEASURED_PEAKS.json.
+value    = m / device time per step (CUDA events on the engine's stream), summed
+           over replicas for N > 1 (a single graph does not shard: N independent
+           replicas, no collective; scaling "weak").
+e2e      = the same metric through the public API from pinned host buffers:
+           each step uploads the CSR (+ device validation), solves and copies
+           the labels back.
+roofline : bytes the decomposition must touch, 2*4(n+1) + 2*4m + 4n (offsets
+           and adjacency of the graph and its transpose once, one u32 label per
+           vertex), divided by the step's device time, against the measured HBM
+           copy bandwidth in MEASURED_PEAKS.json.
+parity   : after the timed region, the labels of the e2e solve are compared
+           bit-exactly with the oracle's restatement of the reference's Tarjan
+           on the same graph.
+workloads: (1 GPU) the other benchmark workloads, each with its own parity,
+           clocks and baseline: the 4096^2 grid, the 4096-graph batch (against
+           one launch per graph and the reference's own GPU FB) and the served
+           stream (plain / batched / batched + network, three repeats).
 --impl reference: the reference's own CPU decomposition (tarjan.cpp
-          TR_Decomposition, compiled from the reference sources into
-          oracle/_ref) on a bounded sample of the workload, rank 0 only.
+           TR_Decomposition, compiled from the reference sources into
+           oracle/_ref) on a bounded sample of the headline workload, rank 0
+           only; the sample is drawn by a numpy restatement of the generator
+           (oracle/rmat_sample.py), so that process loads no product library.
 """
 from __future__ import annotations
 
@@ -42,8 +52,9 @@ METRIC = "SCC edges/s (R-MAT 2^26 / 2^30 samples, scc_2_w -a h, 1 B200)"
 UNIT = "edges/s"
 
 
-def workload_config(scale: int, samples_log2: int, seed: int, extra: dict | None = None) -> dict:
-    cfg = {
+def headline_config(scale: int, samples_log2: int, seed: int, world: int) -> dict:
+    """Workload description shared by both arms (graph statistics go elsewhere)."""
+    return {
         "workload": f"rmat{scale}_e{samples_log2}_scc_2_w_hybrid",
         "graph": f"R-MAT scale {scale}, 2^{samples_log2} samples, (a,b,c,d)=(0.57,0.19,0.19,0.05), "
                  f"ids permuted, self-loops dropped, duplicates merged, seed {seed}",
@@ -51,10 +62,8 @@ def workload_config(scale: int, samples_log2: int, seed: int, extra: dict | None
                 "WCC + trim-2 once, partition rounds",
         "index_dtype": "u32",
         "l2": "inputs larger than L2 (CSR + transpose ~8.6 GB vs 126 MB L2); no flush",
+        "parallelism": f"replicas{world}",
     }
-    if extra:
-        cfg.update(extra)
-    return cfg
 
 
 def b_alg(n: int, m: int) -> int:
@@ -72,7 +81,7 @@ def load_peaks() -> tuple[float, str]:
 
 
 class ClockSampler:
-    """Polls NVML (read-only) every few ms while the timed region runs."""
+    """Polls NVML (read-only) every few ms while a timed region runs."""
 
     def __init__(self, device_index: int, period_s: float = 0.01):
         self.dev = device_index
@@ -112,11 +121,13 @@ class ClockSampler:
         self._stop.set()
         if self._t:
             self._t.join()
+        return self
 
-    def summary(self, t0: float, t1: float) -> dict:
+    def summary(self, t0: float | None = None, t1: float | None = None) -> dict:
         if not self.ok:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvml unavailable"]}
-        win = [s for s in self.samples if t0 <= s[0] <= t1] or self.samples[-3:]
+        win = self.samples if t0 is None else [s for s in self.samples if t0 <= s[0] <= t1]
+        win = win or self.samples[-3:]
         names = {
             0x0000000000000001: "gpu_idle", 0x0000000000000002: "applications_clocks_setting",
             0x0000000000000004: "sw_power_cap", 0x0000000000000008: "hw_slowdown",
@@ -148,83 +159,95 @@ def quiet_stdout():
     return restore
 
 
-def cpu_tarjan_rate(scale: int, seed: int, device: int):
-    """Reference Tarjan (oracle/_ref, else the oracle's port) on a R-MAT sample
-    built on the device -> (edges/s, kind, sample description, seconds)."""
-    import numpy as np
-
-    import gpuscc_code_b200 as scc
+def cpu_tarjan(n, nodes, edges):
+    """The reference's TR_Decomposition (oracle/_ref) or, without it, the
+    oracle's restatement, on one host thread -> (seconds wall, SCC count, kind)."""
     import oracle
 
-    with scc.SCCContext(device) as ctx:
-        ctx.gen_rmat_device(scale, 16 << scale, ABC, seed)
-        g = ctx.download()
     kind = "reference" if oracle.ref_lib() is not None else "port"
     restore = quiet_stdout()
     try:
         t0 = time.perf_counter()
         if kind == "reference":
-            cnt, own = oracle.ref_tarjan(g.n, g.nodes, g.edges)
+            cnt, _ = oracle.ref_tarjan(n, nodes, edges)
         else:
-            _, cnt = oracle.tarjan_labels(g.n, g.nodes, g.edges)
-        wall = time.perf_counter() - t0
+            _, cnt = oracle.tarjan_labels(n, nodes, edges)
+        secs = time.perf_counter() - t0
     finally:
         restore()
-    secs = wall
-    sample = (f"R-MAT scale {scale}, 2^{scale + 4} samples, same (a,b,c,d), permuted, seed {seed}: n={g.n}, "
-              f"m={g.m}, {cnt} SCCs; {'tarjan.cpp TR_Decomposition' if kind == 'reference' else 'oracle port'} "
-              f"on 1 host thread, wall {secs:.2f} s")
-    del np
-    return g.m / secs, kind, sample, secs
+    return secs, cnt, kind
 
 
+def tarjan_parity(graph: str, n: int, nodes, edges, labels, nscc: int, largest: int | None = None) -> dict:
+    """Labels of one solve against the oracle's Tarjan (tarjan.cpp:110-190
+    restated), bit-exact after canonicalisation to minimum ids."""
+    import numpy as np
+
+    import oracle
+
+    t0 = time.perf_counter()
+    ref, rcnt = oracle.tarjan_labels(n, nodes, edges)
+    eq = bool(np.array_equal(np.asarray(labels)[:n + 1], ref))
+    out = {"checked": True, "graph": graph, "oracle": "Tarjan (tarjan.cpp:110-190 restated, oracle/scc_oracle.c)",
+           "labels_equal": eq, "tarjan_count": rcnt, "engine_count": nscc, "counts_equal": rcnt == nscc,
+           "tarjan_largest_scc": int(np.bincount(ref[1:]).max()) if n else 0}
+    if largest is not None:
+        out["engine_largest_scc"] = largest
+    if not eq:
+        out["labels_differing"] = int((np.asarray(labels)[:n + 1] != ref).sum())
+    out["check_s"] = round(time.perf_counter() - t0, 2)
+    return out
+
+
+# ---------------------------------------------------------------- reference
 def run_reference(args) -> None:
     rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
     if rank != 0:
         return
-    import oracle  # noqa: F401
-    import gpuscc_code_b200 as scc
+    if args.workload != "rmat26":
+        print(json.dumps({"impl": "reference", "unavailable": f"the reference arm covers the headline workload; "
+                          f"the {args.workload} workload reports its CPU baseline in its own line"}), flush=True)
+        return
+    import oracle
+    from oracle import rmat_sample
 
     scale = args.ref_scale
-    grid = args.workload == "grid"
-    if grid:
-        g = scc.gen_grid(args.grid_side, 0.15, 0.001, seed=3)
-    else:
-        with scc.SCCContext(0) as ctx:
-            ctx.gen_rmat_device(scale, 16 << scale, ABC, args.seed)
-            g = ctx.download()
+    t0 = time.perf_counter()
+    n, nodes, edges = rmat_sample.rmat_csr(scale, 16 << scale, ABC, args.seed)
+    gen_s = time.perf_counter() - t0
+    m = len(edges)
     kind = "reference" if oracle.ref_lib() is not None else "port"
     times = []
-    restore = quiet_stdout()
-    try:
-        for i in range(args.warmup + args.steps):
-            t0 = time.perf_counter()
-            if kind == "reference":
-                oracle.ref_tarjan(g.n, g.nodes, g.edges)
-            else:
-                oracle.tarjan_labels(g.n, g.nodes, g.edges)
-            if i >= args.warmup:
-                times.append(time.perf_counter() - t0)
-    finally:
-        restore()
+    cnt = None
+    for i in range(args.warmup + args.steps):
+        secs, cnt, _ = cpu_tarjan(n, nodes, edges)
+        if i >= args.warmup:
+            times.append(secs)
     per = sum(times) / len(times)
-    value = g.m / per
-    sample = (f"R-MAT scale {scale}, 2^{scale + 4} samples (same generator, (a,b,c,d), permutation, seed "
-              f"{args.seed}): n={g.n}, m={g.m}; one decomposition per step")
-    metric = METRIC
-    if grid:
-        sample = f"the whole {args.grid_side}^2 grid graph (n={g.n}, m={g.m}); one decomposition per step"
-        metric = f"SCC edges/s ({args.grid_side}x{args.grid_side} grid, 15% bidirectional, scc_2_w -a h, 1 B200)"
+    value = m / per
+    sample = (f"R-MAT scale {scale}, 2^{scale + 4} samples (same generator, (a,b,c,d), permutation and seed "
+              f"{args.seed} as the headline graph, drawn by oracle/rmat_sample.py): n={n}, m={m}, {cnt} SCCs; "
+              f"one {'tarjan.cpp TR_Decomposition' if kind == 'reference' else 'oracle Tarjan'} per step on 1 "
+              f"host thread (the algorithm is sequential); sample built in {gen_s:.1f} s")
     line = {
-        "impl": "reference", "metric": metric, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": per * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-        "config": workload_config(args.scale, args.samples_log2, args.seed,
-                                  {"reference_sample_scale": scale}),
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": kind, "sample": sample},
+        "config": headline_config(args.scale, args.samples_log2, args.seed, world),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": kind, "sample": sample,
+                         "host_cores_available": os.cpu_count()},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ ours
+def pinned_u32(count):
+    import numpy as np
+    import torch
+
+    return torch.empty(int(max(count, 1)), dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
 
 
 def run_ours(args) -> None:
@@ -250,17 +273,8 @@ def run_ours(args) -> None:
         overrides[k] = v if k == "alg" else int(v)
     opts = scc.Options(**{"alg": "h", "wcc": True, "trim2": True, **overrides})
     ctx = scc.SCCContext(local, opts)
-    grid = args.workload == "grid"
-    if grid:
-        # 4096 x 4096 grid, every grid edge oriented by a coin flip, 15 % kept in
-        # both directions, plus random long-range edges numbering 0.1 % of the
-        # grid edges, seed 3 (host generator, then uploaded)
-        gh = scc.gen_grid(args.grid_side, 0.15, 0.001, seed=3)
-        ctx.upload(gh)
-        n, m = int(gh.n), int(gh.m)
-    else:
-        d = ctx.gen_rmat_device(scale, samples, ABC, args.seed)
-        n, m = int(d.n), int(d.m)
+    d = ctx.gen_rmat_device(scale, samples, ABC, args.seed)
+    n, m = int(d.n), int(d.m)
     stream = torch.cuda.ExternalStream(ctx.stream)
     d_labels = torch.zeros(n + 1, dtype=torch.int32, device=f"cuda:{local}")
 
@@ -309,7 +323,7 @@ def run_ours(args) -> None:
     achieved = b_alg(n, m) / (kern_ms / 1e3) / 1e9
     traffic = None
     prof = ROOT / "profiles" / "traffic_rmat_scc_2_w.json"
-    if prof.exists() and not grid:
+    if prof.exists():
         try:
             t = json.loads(prof.read_text())
             traffic = float(t["bytes_per_edge"]) * m + float(t.get("bytes_per_vertex", 0.0)) * n
@@ -318,15 +332,14 @@ def run_ours(args) -> None:
     clocks = sampler.summary(t_wall0, t_wall1)
 
     # e2e through the public API from pinned host buffers
+    h_nodes, h_edges, h_nodesT, h_edgesT = pinned_u32(n + 2), pinned_u32(m), pinned_u32(n + 2), pinned_u32(m)
+    ctx.download_into(h_nodes, h_edges, h_nodesT, h_edgesT)
+    hg = scc.HostCSR.from_arrays(h_nodes, h_edges[:m], h_nodesT, h_edgesT[:m], sorted_unique=True)
+    h_labels = pinned_u32(n + 1)
     e2e = None
+    ctx.upload(hg)  # warm
+    _, c2, st2 = ctx.solve(out=h_labels)
     if not args.no_e2e:
-        pin = lambda cnt_: torch.empty(int(cnt_), dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
-        h_nodes, h_edges, h_nodesT, h_edgesT = pin(n + 2), pin(max(m, 1)), pin(n + 2), pin(max(m, 1))
-        ctx.download_into(h_nodes, h_edges, h_nodesT, h_edgesT)
-        hg = scc.HostCSR.from_arrays(h_nodes, h_edges, h_nodesT, h_edgesT, sorted_unique=True)
-        h_labels = pin(n + 1)
-        ctx.upload(hg)  # warm
-        ctx.solve(out=h_labels)
         if dist:
             dist.barrier()
         torch.cuda.synchronize()
@@ -334,107 +347,212 @@ def run_ours(args) -> None:
         t0 = time.perf_counter()
         for _ in range(e2e_steps):
             ctx.upload(hg)
-            _, c2, _ = ctx.solve(out=h_labels)
+            _, c2, st2 = ctx.solve(out=h_labels)
         torch.cuda.synchronize()
         e2e_s = (time.perf_counter() - t0) / e2e_steps
         if dist:
             t = torch.tensor([e2e_s], dtype=torch.float64, device=f"cuda:{local}")
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             e2e_s = float(t.item())
-        if c2 != cnt:
-            raise SystemExit("e2e SCC count differs from the device-resident run")
         e2e = {"value": world * m / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 2 * 4 * (n + 2) + 2 * 4 * m,
                "d2h_bytes_per_step": 4 * (n + 1), "ms_per_step": e2e_s * 1e3, "steps": e2e_steps}
-
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu and grid:
-        import oracle
-        kind = "reference" if oracle.ref_lib() is not None else "port"
-        restore = quiet_stdout()
-        try:
-            t0 = time.perf_counter()
-            if kind == "reference":
-                oracle.ref_tarjan(gh.n, gh.nodes, gh.edges)
-            else:
-                oracle.tarjan_labels(gh.n, gh.nodes, gh.edges)
-            secs = time.perf_counter() - t0
-        finally:
-            restore()
-        cpu = {"value": m / secs, "unit": UNIT, "cores": 1, "kind": kind, "host_cores_available": os.cpu_count(),
-               "sample": f"the whole grid graph (n={n}, m={m}); "
-                         f"{'tarjan.cpp TR_Decomposition' if kind == 'reference' else 'oracle port'} on 1 host "
-                         f"thread, wall {secs:.2f} s"}
-    elif rank == 0 and world == 1 and not args.no_cpu:
-        rate, kind, sample, _ = cpu_tarjan_rate(args.cpu_scale, args.seed, local)
-        cpu = {"value": rate, "unit": UNIT, "cores": 1, "kind": kind, "sample": sample,
-               "host_cores_available": os.cpu_count()}
-
+    if c2 != cnt:
+        raise SystemExit("e2e SCC count differs from the device-resident run")
+    ctx.close()
     if dist:
         dist.destroy_process_group()
     if rank != 0:
-        ctx.close()
         return
-    if grid:
-        metric = f"SCC edges/s ({args.grid_side}x{args.grid_side} grid, 15% bidirectional, scc_2_w -a {opts.alg}, 1 B200)"
-        data = "synthetic (grid generated on the host, seed 3)"
-        config = {"workload": f"grid{args.grid_side}_bidir15_lr0.1_scc_2_w", "n": n, "m": m, "nscc": cnt,
-                  "graph": f"{args.grid_side}^2 grid, edges oriented at random, 15% bidirectional, long-range "
-                           "edges = 0.1% of grid edges, seed 3",
-                  "index_dtype": "u32", "l2": "inputs larger than L2 (CSR + transpose ~0.4 GB); no flush",
-                  "parallelism": f"replicas{world}", "engine_overrides": overrides,
-                  "rounds": st.get("steps")}
-    else:
-        metric, data = METRIC, "synthetic (R-MAT generated on the device, seed 2)"
-        config = workload_config(scale, args.samples_log2, args.seed,
-                                 {"n": n, "m": m, "nscc": cnt, "parallelism": f"replicas{world}",
-                                  "engine_overrides": overrides})
+
+    parity = None
+    if not args.no_parity:
+        parity = tarjan_parity(f"R-MAT 2^{scale}, 2^{args.samples_log2} samples, seed {args.seed} (the timed graph)",
+                               n, h_nodes, h_edges[:m], h_labels, c2, st2.get("largest_scc"))
+    cpu = None
+    if world == 1 and not args.no_cpu:
+        cpu = cpu_baseline_rmat(args.cpu_scale, args.seed, local)
+    workloads = None
+    if world == 1 and not args.no_workloads:
+        workloads = {}
+        for name, fn in (("grid", measure_grid), ("batch", measure_batch), ("serve", measure_serve)):
+            t0 = time.perf_counter()
+            try:
+                workloads[name] = fn(args)
+            except Exception as e:  # recorded, the headline line still prints
+                workloads[name] = {"error": f"{type(e).__name__}: {e}"}
+            workloads[name]["wall_s"] = round(time.perf_counter() - t0, 1)
+
     line = {
-        "metric": metric, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "u32", "data": data,
-        "config": config,
+        "vs_baseline": None, "dtype": "u32", "data": "synthetic (R-MAT generated on the device, seed 2)",
+        "config": headline_config(scale, args.samples_log2, args.seed, world),
+        "graph_stats": {"n": n, "m": m, "nscc": cnt, "largest_scc": st2.get("largest_scc"),
+                        "rounds": st.get("steps")},
+        "engine_overrides": overrides,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
-                     "kernel": "scc_persistent<256> (+ per-step init pass)", "kernel_ms": kern_ms,
+                     "kernel": f"scc_persistent<{opts.block_size}> (+ per-step init pass)", "kernel_ms": kern_ms,
                      "algorithmic_bytes": b_alg(n, m)},
         "clocks": clocks,
         "gpu_launches": launches,
         "e2e": e2e,
         "cpu_baseline": cpu,
+        "parity": parity,
+        "workloads": workloads,
         "stats": {k: (round(v, 4) if isinstance(v, float) else v) for k, v in st.items()},
         "profile_ms": {k: v for k, v in prof_last.items()},
         "trace": trace_last if args.trace else None,
     }
     print(json.dumps(line), flush=True)
+
+
+def cpu_baseline_rmat(scale: int, seed: int, device: int) -> dict:
+    """Reference Tarjan on a R-MAT sample of the headline workload (built on the device)."""
+    import gpuscc_code_b200 as scc
+
+    with scc.SCCContext(device) as ctx:
+        ctx.gen_rmat_device(scale, 16 << scale, ABC, seed)
+        g = ctx.download()
+    secs, cnt, kind = cpu_tarjan(g.n, g.nodes, g.edges)
+    return {"value": g.m / secs, "unit": UNIT, "cores": 1, "kind": kind, "host_cores_available": os.cpu_count(),
+            "sample": f"R-MAT scale {scale}, 2^{scale + 4} samples, same (a,b,c,d), permuted, seed {seed}: "
+                      f"n={g.n}, m={g.m}, {cnt} SCCs; "
+                      f"{'tarjan.cpp TR_Decomposition' if kind == 'reference' else 'oracle port'} on 1 host "
+                      f"thread, wall {secs:.2f} s"}
+
+
+# ------------------------------------------------------------- workloads
+def _events_ms(stream, fn, steps: int):
+    """Device ms of each of `steps` calls of fn() (CUDA events on `stream`)."""
+    import torch
+
+    out = []
+    for _ in range(steps):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        fn()
+        b.record(stream)
+        b.synchronize()
+        out.append(a.elapsed_time(b))
+    return out
+
+
+def measure_grid(args) -> dict:
+    """4096^2 grid (config 3): every grid edge oriented by a coin flip, 15 %
+    kept in both directions, long-range edges numbering 0.1 % of the grid
+    edges, seed 3; scc_2_w -a h; device time per solve, end to end through
+    scc_solve from pinned buffers, the reference Tarjan, parity."""
+    import torch
+
+    import gpuscc_code_b200 as scc
+
+    side = args.grid_side
+    gh = scc.gen_grid(side, 0.15, 0.001, seed=3)
+    n, m = gh.n, gh.m
+    ctx = scc.SCCContext(0, scc.Options(alg="h", wcc=True, trim2=True))
+    ctx.upload(gh)
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    for _ in range(3):
+        cnt, st = ctx.solve_device()
+    sampler = ClockSampler(0).start()
+    ms = _events_ms(stream, lambda: ctx.solve_enqueue(), args.workload_steps)
+    cnt, st = ctx.solve_collect()
+    clocks = sampler.stop().summary()
+    prof = ctx.profile()
+    dev_ms = statistics.median(ms)
+    # end to end: pinned graph up, solve, labels down
+    arrs = [pinned_u32(n + 2), pinned_u32(m), pinned_u32(n + 2), pinned_u32(m)]
+    for a, src in zip(arrs, (gh.nodes, gh.edges, gh.nodesT, gh.edgesT)):
+        a[:len(src)] = src
+    hp = scc.HostCSR.from_arrays(arrs[0], arrs[1][:m], arrs[2], arrs[3][:m], sorted_unique=True)
+    out = pinned_u32(n + 1)
+    ctx.upload(hp)
+    ctx.solve(out=out)
+    t0 = time.perf_counter()
+    reps = 3
+    for _ in range(reps):
+        ctx.upload(hp)
+        _, c2, st2 = ctx.solve(out=out)
+    e2e_s = (time.perf_counter() - t0) / reps
     ctx.close()
+    peak, peak_kind = load_peaks()
+    achieved = b_alg(n, m) / (dev_ms / 1e3) / 1e9
+    secs, rcnt, kind = cpu_tarjan(n, gh.nodes, gh.edges)
+    return {
+        "metric": f"SCC edges/s ({side}x{side} grid, 15% bidirectional, scc_2_w -a h)",
+        "value": m / (dev_ms / 1e3), "unit": UNIT, "ms_per_step": dev_ms, "steps": len(ms),
+        "ms_all": [round(x, 3) for x in ms],
+        "config": {"workload": f"grid{side}_bidir15_lr0.1_scc_2_w", "n": n, "m": m, "nscc": cnt,
+                   "rounds": st.get("steps"), "l2": "inputs larger than L2 (CSR + transpose 0.44 GB); no flush"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_kind": peak_kind, "algorithmic_bytes": b_alg(n, m)},
+        "e2e": {"value": m / e2e_s, "unit": UNIT, "ms_per_step": e2e_s * 1e3,
+                "h2d_bytes_per_step": 8 * (n + 2) + 8 * m, "d2h_bytes_per_step": 4 * (n + 1)},
+        "cpu_baseline": {"value": m / secs, "unit": UNIT, "cores": 1, "kind": kind, "count": rcnt,
+                         "sample": "the whole grid graph, one Tarjan on 1 host thread"},
+        "parity": tarjan_parity(f"grid {side}^2, seed 3", n, gh.nodes, gh.edges, out, c2, st2.get("largest_scc")),
+        "clocks": clocks, "profile_ms": prof, "gpu_launches": 2 * len(ms),
+    }
 
 
-def run_batch(args) -> None:
+def _local_graph(nodes, edges, nodesT, edgesT, lo, hi):
+    """Graph on global ids lo .. hi-1 of a packed batch, in local ids (reference layout)."""
+    import numpy as np
+
+    e0, e1 = int(nodes[lo]), int(nodes[hi])
+    t0, t1 = int(nodesT[lo]), int(nodesT[hi])
+    k = hi - lo
+    ln = np.zeros(k + 2, np.uint32)
+    ln[1:] = nodes[lo:hi + 1] - e0
+    lt = np.zeros(k + 2, np.uint32)
+    lt[1:] = nodesT[lo:hi + 1] - t0
+    return ln, edges[e0:e1] - np.uint32(lo - 1), lt, edgesT[t0:t1] - np.uint32(lo - 1)
+
+
+def _batch_parity(labels, seg, nodes, edges, nodesT, edgesT) -> dict:
+    """Every graph of a packed batch against the oracle's Tarjan, host threads side by side."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    import numpy as np
+
+    import oracle
+
+    t0 = time.perf_counter()
+
+    def one(gi):
+        lo, hi = int(seg[gi]), int(seg[gi + 1])
+        ln, le, _, _ = _local_graph(nodes, edges, nodesT, edgesT, lo, hi)
+        ref, rcnt = oracle.tarjan_labels(hi - lo, ln, le)
+        mine = np.zeros(hi - lo + 1, np.uint32)
+        mine[1:] = labels[lo:hi] - np.uint32(lo - 1)
+        return rcnt, bool(np.array_equal(mine, ref))
+
+    with ThreadPoolExecutor(max_workers=min(32, os.cpu_count() or 1)) as ex:
+        res = list(ex.map(one, range(len(seg) - 1)))
+    bad = [i for i, (_, ok) in enumerate(res) if not ok]
+    return {"checked": True, "graphs": len(res), "graphs_equal": len(res) - len(bad), "labels_equal": not bad,
+            "first_differing": bad[:5], "tarjan_count": sum(c for c, _ in res),
+            "oracle": "Tarjan (tarjan.cpp:110-190 restated) per graph", "check_s": round(time.perf_counter() - t0, 1)}
+
+
+def measure_batch(args, rank: int = 0) -> dict:
     """4096 independent graphs (ER / R-MAT 50/50, n log-uniform in [1e3, 2e5],
     average out-degree U[2, 16], seed 4) packed into one segmented CSR and
     solved by one persistent launch replayed from a captured CUDA graph, with
     parameters from the autotuner; against the same graphs solved one launch
-    per graph (upload + solve each, the plain way)."""
+    per graph (upload + solve each) and the reference's own GPU FB."""
+    import subprocess
+
     import numpy as np
     import torch
 
     import gpuscc_code_b200 as scc
     from gpuscc_code_b200 import autotune
+    from oracle import ref_gpu
 
     count = args.batch_count
-    # under torchrun every rank solves a batch of its own (seed 4 + rank) on
-    # its GPU: independent graphs, no collective on the data path (weak scaling)
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    ctx = scc.SCCContext(local, scc.Options(alg="h", wcc=True, trim2=True))
+    ctx = scc.SCCContext(0, scc.Options(alg="h", wcc=True, trim2=True))
     seg = ctx.gen_batch_device(count, 1000, 200_000, 2.0, 16.0, seed=4 + rank)
     n, m = ctx.n, ctx.m
     tuned, trials = ctx.options, []
@@ -443,106 +561,86 @@ def run_batch(args) -> None:
                  "switch_permille": [10, 50]}
         tuned, trials = autotune.autotune(ctx, space=space, repeats=2)
     ctx.capture()
-    for _ in range(args.warmup):
+    for _ in range(3):
         ctx.replay()
     stream = torch.cuda.ExternalStream(ctx.stream)
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    torch.cuda.synchronize()
-    ms_dev = []
-    if dist:
-        dist.barrier()
-    for _ in range(args.steps):
-        ev0.record(stream)
-        cnt, st = ctx.replay()
-        ev1.record(stream)
-        ev1.synchronize()
-        ms_dev.append(ev0.elapsed_time(ev1))
-    batched_ms = statistics.median(ms_dev)
-    batch_profile = ctx.profile()  # device phase timers of the last replay
-    batch_stats = st
-    if dist:
-        t = torch.tensor([batched_ms], dtype=torch.float64, device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        batched_ms = float(t.item())
-        dist.destroy_process_group()
-        if rank != 0:
-            ctx.close()
-            return
-        line = {
-            "metric": "batched SCC graphs/s (4096 mixed ER/R-MAT graphs per GPU, one launch each)",
-            "value": world * count / (batched_ms / 1e3), "unit": "graphs/s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": batched_ms, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "u32", "data": "synthetic (one batch per rank, seed 4 + rank)",
-            "config": {"workload": f"batch{count}_er_rmat_n1e3-2e5_deg2-16", "graphs_per_gpu": count,
-                       "parallelism": f"independent batches x{world}", "l2": "inputs larger than L2"},
-            "gpu_launches": 2 * args.steps, "profile_ms": batch_profile,
-        }
-        print(json.dumps(line), flush=True)
-        ctx.close()
-        return
-    # the same graphs, one launch each (local ids, uploaded and solved one by one)
+    sampler = ClockSampler(0).start()
+    res = {}
+    ms = _events_ms(stream, lambda: res.update(r=ctx.replay()), args.workload_steps)
+    clocks = sampler.stop().summary()
+    cnt, st = res["r"]
+    prof = ctx.profile()
+    labels = ctx.read_labels()
+    batched_ms = statistics.median(ms)
     full = ctx.download()
+    ctx.close()
     nodes, edges, nodesT, edgesT = (np.asarray(a) for a in (full.nodes, full.edges, full.nodesT, full.edgesT))
+    # the same graphs, one launch each (local ids, uploaded and solved one by one)
+    graphs = [scc.HostCSR.from_arrays(*_local_graph(nodes, edges, nodesT, edgesT, int(seg[g]), int(seg[g + 1])),
+                                      sorted_unique=True) for g in range(count)]
     per = scc.SCCContext(0, scc.Options(alg="h", wcc=True, trim2=True))
-    locals_ = []
-    for g in range(count):
-        lo, hi = int(seg[g]), int(seg[g + 1])  # global ids lo .. hi-1
-        e0, e1 = int(nodes[lo]), int(nodes[hi])
-        t0_, t1_ = int(nodesT[lo]), int(nodesT[hi])
-        k = hi - lo
-        ln = np.zeros(k + 2, np.uint32)
-        ln[1:] = nodes[lo:hi + 1] - e0
-        lt = np.zeros(k + 2, np.uint32)
-        lt[1:] = nodesT[lo:hi + 1] - t0_
-        locals_.append(scc.HostCSR.from_arrays(ln, edges[e0:e1] - (lo - 1), lt, edgesT[t0_:t1_] - (lo - 1),
-                                               sorted_unique=True))
-    per.upload(locals_[0])
+    per.upload(graphs[0])
     per.solve()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    dev_sum = 0.0
-    total_cnt = 0
-    for hg in locals_:
+    dev_sum, total_cnt = 0.0, 0
+    for hg in graphs:
         per.upload(hg)
         _, c, s2 = per.solve(want_labels=False)
         dev_sum += s2["ms_total"]
         total_cnt += c
     wall = time.perf_counter() - t0
-    if total_cnt != cnt:
-        raise SystemExit(f"per-graph SCC total {total_cnt} differs from the batched count {cnt}")
-    line = {
-        "metric": "batched SCC graphs/s (4096 mixed ER/R-MAT graphs, one launch)", "value": count / (batched_ms / 1e3),
-        "unit": "graphs/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": batched_ms,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
-        "data": "synthetic (batch generated on the device, seed 4)",
-        "config": {"workload": f"batch{count}_er_rmat_n1e3-2e5_deg2-16", "n": n, "m": m, "nscc": cnt,
-                   "graphs": count, "launch": "captured CUDA graph: reset + init + one cooperative persistent kernel",
-                   "l2": "inputs larger than L2"},
+    per.close()
+    del graphs
+    gps = count / (batched_ms / 1e3)
+    out = {
+        "metric": f"batched SCC graphs/s ({count} mixed ER/R-MAT graphs, one captured launch)",
+        "value": gps, "unit": "graphs/s", "ms_per_step": batched_ms, "steps": len(ms),
+        "ms_all": [round(x, 3) for x in ms],
+        "config": {"workload": f"batch{count}_er_rmat_n1e3-2e5_deg2-16", "n": n, "m": m, "nscc": cnt, "graphs": count,
+                   "launch": "captured CUDA graph: reset + init + one cooperative persistent kernel",
+                   "l2": "inputs larger than L2 (packed CSR + transpose ~11 GB); no flush"},
         "tuned": {k: getattr(tuned, k) for k in ("block_size", "occupancy", "heavy_degree", "pull_alpha",
                                                  "pull_beta", "switch_permille")},
-        "tuning_trials": [[f, v, round(ms, 3)] for f, v, ms in trials],
-        "per_graph_baseline": {"graphs_per_s_wall": count / wall, "graphs_per_s_device": count / (dev_sum / 1e3),
-                               "ms_device_sum": dev_sum, "s_wall": wall,
-                               "how": "one upload + one scc_solve per graph, same options, local ids"},
-        "speedup_vs_per_graph": {"wall": (count / (batched_ms / 1e3)) / (count / wall),
-                                 "device": dev_sum / batched_ms},
-        "gpu_launches": 2 * args.steps,
-        "profile_ms": batch_profile,
-        "stats": {k: (round(v, 4) if isinstance(v, float) else v) for k, v in batch_stats.items()},
+        "tuning_trials": [[f, v, round(t, 3)] for f, v, t in trials],
+        "per_graph_plain": {"graphs_per_s_wall": count / wall, "graphs_per_s_device": count / (dev_sum / 1e3),
+                            "count_equal": total_cnt == cnt,
+                            "how": "this engine, one upload + one scc_solve per graph, same options, local ids"},
+        "speedup_vs_per_graph": {"wall": gps / (count / wall), "device": dev_sum / batched_ms},
+        "clocks": clocks, "profile_ms": prof, "gpu_launches": 2 * len(ms),
+        "stats": {k: (round(v, 4) if isinstance(v, float) else v) for k, v in st.items()},
     }
-    print(json.dumps(line), flush=True)
-    per.close()
-    ctx.close()
+    # the reference's own GPU FB on the first graphs of the same batch, one at a time (child process)
+    if ref_gpu.available() and args.refgpu_batch > 0:
+        try:
+            r = subprocess.run([sys.executable, "-m", "oracle.ref_gpu", "--batch", str(args.refgpu_batch), "--alg",
+                                "h"], cwd=ROOT, capture_output=True, text=True, timeout=args.refgpu_timeout)
+            ref = json.loads(r.stdout.strip().splitlines()[-1]) if r.returncode == 0 else {
+                "error": f"exit {r.returncode}: {(r.stderr or r.stdout).strip()[-200:]}"}
+        except subprocess.TimeoutExpired:
+            ref = {"error": f"no result within {args.refgpu_timeout} s"}
+        if "graphs_per_s_timer" in ref:
+            ref["speedup_of_batched"] = {"vs_timer": gps / ref["graphs_per_s_timer"],
+                                         "vs_wall": gps / ref["graphs_per_s_wall"]}
+        out["reference_gpu_fb"] = ref
+    else:
+        out["reference_gpu_fb"] = {"unavailable": "oracle/_ref/libscc_ref_gpu.so not built"}
+    if not args.no_parity:
+        out["parity"] = _batch_parity(labels, seg, nodes, edges, nodesT, edgesT)
+        out["parity"]["counts_equal"] = out["parity"]["tarjan_count"] == cnt
+    return out
 
 
-def run_serve(args) -> None:
-    """Served stream: Poisson arrivals of R-MAT (scale 14-22, average degree
-    8-32) and grid graphs (side 256-2048, 10-30 % bidirectional), seed 5.
-    A pool of distinct graphs is generated first and the stream cycles
-    through it.  Three arms serve the same arrival sequence: the plain
-    hybrid one graph per launch, continuous batching, and continuous batching
-    with the trained strategy network.  Every request's labels are compared
-    with the same graph solved alone by the plain method."""
+def measure_serve(args) -> dict:
+    """Served stream (config 5): Poisson arrivals of R-MAT (scale 14-22,
+    average degree 8-32) and grid graphs (side 256-2048, 10-30 %
+    bidirectional), seed 5.  The graphs are registered with the server first
+    (their CSR stays resident on the device); each request names a graph.
+    Three arms serve the same arrival sequence: the plain hybrid one graph per
+    launch, continuous batching, and continuous batching with the trained
+    strategy network; each is run `serve_repeats` times.  Every request's
+    labels are compared with the same graph solved alone by the plain method,
+    and those with the oracle's Tarjan."""
     import numpy as np
     import torch
 
@@ -550,40 +648,23 @@ def run_serve(args) -> None:
     from gpuscc_code_b200 import learned
     from gpuscc_code_b200.serve import Server, make_graph, poisson_arrivals, run_stream, stream_spec
 
-    torch.cuda.set_device(0)
     base = scc.Options(alg="h", wcc=True, trim2=True)
     ctx = scc.SCCContext(0, base)
-
-    def pinned(count):
-        return torch.empty(int(count), dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
-
-    # clients hand over page-locked buffers (graph arrays and label outputs)
-    pool = []
-    for i in range(args.serve_pool):
-        g = make_graph(stream_spec(i, seed=5), ctx)
-        a = [pinned(g.n + 2), pinned(max(g.m, 1)), pinned(g.n + 2), pinned(max(g.m, 1))]
-        a[0][:] = g.nodes
-        a[1][:g.m] = g.edges
-        a[2][:] = g.nodesT
-        a[3][:g.m] = g.edgesT
-        pool.append(scc.HostCSR.from_arrays(a[0], a[1][:g.m], a[2], a[3][:g.m], sorted_unique=True))
-        del g
-    # alone: plain method, one graph at a time, upload + solve + labels back (the
-    # labels every arm must reproduce, and the service time that sets the rate)
+    pool = [make_graph(stream_spec(i, seed=5), ctx) for i in range(args.serve_pool)]
+    # alone: plain method, one graph at a time (the labels every arm must reproduce)
     alone, svc_ms = [], []
     for g in pool:
-        out = pinned(g.n + 1)
-        t0 = time.perf_counter()
         ctx.upload(g)
-        ctx.solve(out=out)
-        svc_ms.append((time.perf_counter() - t0) * 1e3)
-        alone.append(out.copy())
+        labels, _, st = ctx.solve()
+        svc_ms.append(st["ms_total"])
+        alone.append(labels)
     ctx.close()
-    reqs = [pool[i % len(pool)] for i in range(args.serve_requests)]
-    ref = [alone[i % len(pool)] for i in range(args.serve_requests)]
-    outs = [pinned(g.n + 1) for g in reqs]
+    oracle_ok = all(np.array_equal(a, __import__("oracle").tarjan_labels(g.n, g.nodes, g.edges)[0])
+                    for g, a in zip(pool, alone))
+    reqs = [i % len(pool) for i in range(args.serve_requests)]
+    outs = [pinned_u32(pool[i].n + 1) for i in reqs]
     rate = args.serve_rate
-    if rate <= 0:  # load the plain server close to its end-to-end capacity
+    if rate <= 0:  # load the plain server close to its device capacity
         rate = 0.9 * 1e3 / float(np.mean(svc_ms))
     arrivals = poisson_arrivals(len(reqs), rate, seed=5)
     model = learned.DEFAULT_MODEL if learned.DEFAULT_MODEL.exists() else None
@@ -591,58 +672,110 @@ def run_serve(args) -> None:
     if model is not None:
         arms.append(("batched_learned", dict(batching=True), model))
     out = {}
+    exact_all = True
     for name, kw, mdl in arms:
-        with Server(0, base, model=mdl, **kw) as srv:
-            # capacity: every request at once (the server is never idle), after
-            # one unmeasured burst that grows the server's memory pool
-            run_stream(srv, reqs, np.zeros(len(reqs)), outs)
-            burst = run_stream(srv, reqs, np.zeros(len(reqs)), outs)
-            exact_burst = all(np.array_equal(a[:len(b)], b) for a, b in zip(burst["labels"], ref))
-            st0 = srv.stats()
-            res = run_stream(srv, reqs, arrivals, outs)
-            st = srv.stats()
-            st["batches"] -= st0["batches"]
-        exact = all(np.array_equal(a[:len(b)], b) for a, b in zip(res["labels"], ref)) and exact_burst
-        if not exact:
-            raise SystemExit(f"serve arm {name}: labels differ from the graph solved alone")
-        picks = {}
-        for info in res["info"]:
-            picks[str(info["choice"])] = picks.get(str(info["choice"]), 0) + 1
-        out[name] = {"graphs_per_s": res["graphs_per_s"], "p50_ms": res["p50_ms"], "p99_ms": res["p99_ms"],
-                     "capacity_graphs_per_s": burst["graphs_per_s"],
-                     "mean_batch": float(np.mean([i["batch_graphs"] for i in res["info"]])),
-                     "batches": st["batches"], "labels_exact": exact,
-                     "peak_resident_bytes": st["peak_resident_bytes"], "choices": picks}
-        del res
-    best = max(out.values(), key=lambda a: a["capacity_graphs_per_s"])
-    n_tot = sum(int(g.n) for g in reqs)
-    m_tot = sum(int(g.m) for g in reqs)
-    line = {
-        "metric": "served SCC graphs/s (Poisson stream of R-MAT + grid graphs, p50/p99 latency)",
-        "value": best["capacity_graphs_per_s"], "unit": "graphs/s", "n_gpus": 1, "steps": 1, "warmup": 1,
-        "ms_per_step": 1e3 * len(reqs) / best["capacity_graphs_per_s"], "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "u32", "data": "synthetic (stream generated in-process, seed 5)",
-        "config": {"workload": f"serve{len(reqs)}_pool{len(pool)}_rmat14-22_grid256-2048",
-                   "requests": len(reqs), "distinct_graphs": len(pool), "rate_per_s": rate,
-                   "vertices": n_tot, "edges": m_tot, "model": str(model.name) if model else None},
+        reps = []
+        for rep in range(args.serve_repeats):
+            with Server(0, base, model=mdl, **kw) as srv:
+                handles = [srv.register(g) for g in pool]
+                items = [handles[i] for i in reqs]
+                run_stream(srv, items[:len(pool)], np.zeros(len(pool)), outs[:len(pool)])  # warm the pools
+                burst = run_stream(srv, items, np.zeros(len(items)), outs)
+                exact = all(np.array_equal(a[:len(alone[i])], alone[i]) for a, i in zip(burst["labels"], reqs))
+                st0 = srv.stats()
+                res = run_stream(srv, items, arrivals, outs)
+                st = srv.stats()
+            exact = exact and all(np.array_equal(a[:len(alone[i])], alone[i]) for a, i in zip(res["labels"], reqs))
+            exact_all &= exact
+            picks = {}
+            for info in res["info"]:
+                picks[str(info["choice"])] = picks.get(str(info["choice"]), 0) + 1
+            reps.append({"capacity_graphs_per_s": burst["graphs_per_s"], "graphs_per_s": res["graphs_per_s"],
+                         "p50_ms": res["p50_ms"], "p99_ms": res["p99_ms"],
+                         "mean_batch": float(np.mean([i["batch_graphs"] for i in res["info"]])),
+                         "batches": st["batches"] - st0["batches"], "labels_exact": exact, "choices": picks})
+        agg = {}
+        for key in ("capacity_graphs_per_s", "graphs_per_s", "p50_ms", "p99_ms"):
+            v = [r[key] for r in reps]
+            agg[key] = {"min": min(v), "median": statistics.median(v), "max": max(v)}
+        out[name] = {"summary": agg, "repeats": reps}
+    med = lambda arm, key: out[arm]["summary"][key]["median"]
+    return {
+        "metric": "served SCC graphs/s (Poisson stream of R-MAT + grid graphs, resident CSR, p50/p99 latency)",
+        "value": max(med(a, "capacity_graphs_per_s") for a in out), "unit": "graphs/s",
+        "config": {"workload": f"serve{len(reqs)}_pool{len(pool)}_rmat14-22_grid256-2048", "requests": len(reqs),
+                   "distinct_graphs": len(pool), "rate_per_s": rate, "repeats": args.serve_repeats,
+                   "vertices": int(sum(pool[i].n for i in reqs)), "edges": int(sum(pool[i].m for i in reqs)),
+                   "model": str(model.name) if model else None},
         "arms": out,
-        "capacity_vs_plain": {k: v["capacity_graphs_per_s"] / out["plain"]["capacity_graphs_per_s"]
-                              for k, v in out.items()},
-        "p99_vs_plain": {k: out["plain"]["p99_ms"] / v["p99_ms"] for k, v in out.items()},
-        "plain_mean_service_ms": float(np.mean(svc_ms)),
-        "note": "graphs and label buffers in page-locked host memory; service time = upload + solve + labels "
-                "back, one graph alone; rate = 0.9 / mean service time unless given; p50/p99 at that rate; "
-                "capacity = the same requests submitted at once, after one unmeasured such burst that grows the "
-                "server's memory pool; value = the best arm's capacity",
+        "capacity_vs_plain": {a: med(a, "capacity_graphs_per_s") / med("plain", "capacity_graphs_per_s") for a in out},
+        "p99_vs_plain": {a: med("plain", "p99_ms") / med(a, "p99_ms") for a in out},
+        "plain_mean_device_ms": float(np.mean(svc_ms)),
+        "parity": {"checked": True, "labels_equal": bool(exact_all and oracle_ok),
+                   "how": "every request's labels equal the graph solved alone by the plain method, and those "
+                          "equal the oracle's Tarjan"},
+        "note": "graphs registered with the server before the stream (CSR resident on the device); each request "
+                "names a graph and receives its labels in page-locked host memory; rate = 0.9 / mean plain device "
+                "time unless given; capacity = all requests submitted at once; value = best arm's median capacity",
     }
-    print(json.dumps(line), flush=True)
+
+
+def run_workload(args) -> None:
+    import torch
+
+    torch.cuda.set_device(0)
+    fn = {"grid": measure_grid, "batch": measure_batch, "serve": measure_serve}[args.workload]
+    res = fn(args)
+    res.setdefault("n_gpus", 1)
+    print(json.dumps(res), flush=True)
+
+
+def run_batch_multi(args) -> None:
+    """--workload batch under torchrun: every rank solves a batch of its own
+    (seed 4 + rank) on its GPU (independent graphs, no collective on the data
+    path); the line reports N x graphs / the slowest rank's time."""
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ["WORLD_SIZE"])
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    import gpuscc_code_b200 as scc
+
+    ctx = scc.SCCContext(local, scc.Options(alg="h", wcc=True, trim2=True, block_size=512, heavy_degree=1024,
+                                            pull_alpha=6, switch_permille=50))
+    ctx.gen_batch_device(args.batch_count, 1000, 200_000, 2.0, 16.0, seed=4 + rank)
+    ctx.capture()
+    for _ in range(args.warmup):
+        ctx.replay()
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    dist.barrier()
+    ms = statistics.median(_events_ms(stream, ctx.replay, args.steps))
+    t = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{local}")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ctx.close()
+    dist.destroy_process_group()
+    if rank == 0:
+        ms = float(t.item())
+        print(json.dumps({
+            "metric": "batched SCC graphs/s (mixed ER/R-MAT graphs per GPU, one launch each)",
+            "value": world * args.batch_count / (ms / 1e3), "unit": "graphs/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u32", "data": "synthetic (one batch per rank, seed 4 + rank)",
+            "config": {"workload": f"batch{args.batch_count}_er_rmat_n1e3-2e5_deg2-16",
+                       "parallelism": f"independent batches x{world}", "l2": "inputs larger than L2"},
+            "gpu_launches": 2 * args.steps}), flush=True)
 
 
 def run_refgpu(args) -> None:
     """The reference's own GPU FB (scc_2_w build, compiled from its sources for
     sm_100a into oracle/_ref) against this engine on the same graphs and the
     same device: R-MAT scale 16 / 2^20 samples (seed 1, config 1), R-MAT at
-    larger scales (seed 2) and a grid.  The reference runs in a child process
+    larger scales (seed 2) and grids.  The reference runs in a child process
     (it prints and exit()s on errors) under a time limit; both sides report the
     solve time from a resident CSR (the reference's own timer, scc.cu:217-1011;
     CUDA events here) and the SCC count, which must agree."""
@@ -663,7 +796,9 @@ def run_refgpu(args) -> None:
     for sc in args.refgpu_scales:
         cases.append((f"rmat{sc}_e{sc + 4}_seed2", ["--rmat", str(sc), "--samples-log2", str(sc + 4), "--seed", "2"],
                       lambda c, sc=sc: c.gen_rmat_device(sc, 1 << (sc + 4), seed=2)))
-    cases.append((f"grid{args.refgpu_grid}_seed3", ["--grid", str(args.refgpu_grid), "--seed", "3"], None))
+    for side in args.refgpu_grids:
+        cases.append((f"grid{side}_seed3", ["--grid", str(side), "--seed", "3"],
+                      lambda c, side=side: c.upload(scc.gen_grid(side, 0.15, 0.001, seed=3))))
     rows = []
     for name, cli, gen in cases:
         row = {"graph": name}
@@ -677,10 +812,7 @@ def run_refgpu(args) -> None:
                 ref = {"error": f"no result within {args.refgpu_timeout} s"}
             row[f"reference_{alg}"] = ref
         ctx = scc.SCCContext(0, scc.Options(alg="h", wcc=True, trim2=True))
-        if gen is None:
-            ctx.upload(scc.gen_grid(args.refgpu_grid, 0.15, 0.001, seed=3))
-        else:
-            gen(ctx)
+        gen(ctx)
         for _ in range(3):
             cnt, st = ctx.solve_device()
         ms = []
@@ -695,33 +827,8 @@ def run_refgpu(args) -> None:
                 ref["count_matches"] = ref["nscc"] == cnt
                 ref["speedup_of_ours"] = ref["secs"] / row["ours_h"]["secs"]
         rows.append(row)
-    # the mixed batch: the reference solves graphs one at a time (a sample of
-    # them), the engine all 4096 in one captured launch
-    batch = {"graphs": 4096, "reference_sample": args.refgpu_batch}
-    try:
-        r = subprocess.run([sys.executable, "-m", "oracle.ref_gpu", "--batch", str(args.refgpu_batch), "--alg", "h"],
-                           cwd=ROOT, capture_output=True, text=True, timeout=args.refgpu_timeout)
-        batch["reference_h"] = json.loads(r.stdout.strip().splitlines()[-1]) if r.returncode == 0 else {
-            "error": f"exit {r.returncode}: {(r.stderr or r.stdout).strip()[-200:]}"}
-    except subprocess.TimeoutExpired:
-        batch["reference_h"] = {"error": f"no result within {args.refgpu_timeout} s"}
-    ctx = scc.SCCContext(0, scc.Options(alg="h", wcc=True, trim2=True))
-    ctx.gen_batch_device(4096, 1000, 200_000, 2.0, 16.0, seed=4)
-    ctx.capture()
-    for _ in range(3):
-        ctx.replay()
-    ms = []
-    for _ in range(5):
-        _, st = ctx.replay()
-        ms.append(st["ms_total"])
-    ctx.close()
-    batch["ours_batched_graphs_per_s"] = 4096 / (statistics.median(ms) / 1e3)
-    ref = batch["reference_h"]
-    if "graphs_per_s_timer" in ref:
-        batch["speedup_vs_reference_timer"] = batch["ours_batched_graphs_per_s"] / ref["graphs_per_s_timer"]
-        batch["speedup_vs_reference_wall"] = batch["ours_batched_graphs_per_s"] / ref["graphs_per_s_wall"]
     print(json.dumps({"metric": "SCC solve time vs the reference's GPU FB (same B200, same graphs)",
-                      "unit": "s", "rows": rows, "batch": batch,
+                      "unit": "s", "rows": rows,
                       "note": "reference: scc.cu computeSCC of the scc_2_w build (-DWCC -DTRIM_2), its own timer; "
                               "ours: scc_2_w -a h, CUDA events, median of 5"}), flush=True)
 
@@ -740,22 +847,25 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-parity", action="store_true", help="skip the Tarjan label checks")
+    ap.add_argument("--no-workloads", action="store_true", help="headline line only")
+    ap.add_argument("--workload-steps", type=int, default=10, help="timed steps of each workload")
     ap.add_argument("--trace", action="store_true", help="include the per-sweep device trace in the line")
     ap.add_argument("--opt", action="append", default=[], metavar="KEY=VALUE",
                     help="override an engine option (scc_opts field), e.g. --opt occupancy=3")
     ap.add_argument("--grid-side", type=int, default=4096, help="grid: side of the grid graph")
     ap.add_argument("--refgpu-scales", type=int, nargs="*", default=[20, 22],
                     help="refgpu: further R-MAT scales (2^(scale+4) samples, seed 2)")
-    ap.add_argument("--refgpu-grid", type=int, default=1024, help="refgpu: grid side")
+    ap.add_argument("--refgpu-grids", type=int, nargs="*", default=[1024, 4096], help="refgpu: grid sides")
     ap.add_argument("--refgpu-algs", nargs="*", default=["h", "t"], help="refgpu: reference -a arms")
     ap.add_argument("--refgpu-timeout", type=int, default=300)
-    ap.add_argument("--refgpu-batch", type=int, default=256, help="refgpu: batch graphs the reference solves")
+    ap.add_argument("--refgpu-batch", type=int, default=256, help="batch: graphs the reference GPU FB solves")
     ap.add_argument("--workload", choices=["rmat26", "grid", "batch", "serve", "refgpu"], default="rmat26",
-                    help="rmat26: the headline line; batch: 4096 packed graphs in one launch vs one launch each; "
-                         "serve: Poisson stream through the request loop (plain / batched / batched + network); "
-                         "grid: the 4096^2 high-diameter grid graph")
-    ap.add_argument("--serve-pool", type=int, default=48, help="serve: distinct graphs in the stream")
-    ap.add_argument("--serve-requests", type=int, default=240, help="serve: requests in the stream")
+                    help="rmat26: the headline line (with the other workloads inside it); grid / batch / serve: "
+                         "one workload alone; refgpu: the reference's GPU FB on the same graphs")
+    ap.add_argument("--serve-pool", type=int, default=24, help="serve: distinct graphs in the stream")
+    ap.add_argument("--serve-requests", type=int, default=96, help="serve: requests in the stream")
+    ap.add_argument("--serve-repeats", type=int, default=3)
     ap.add_argument("--serve-rate", type=float, default=0.0,
                     help="serve: arrivals per second (0 = 0.9 x the plain method's device throughput)")
     ap.add_argument("--batch-count", type=int, default=4096)
@@ -763,21 +873,16 @@ def main():
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
-    if args.workload == "refgpu":
-        if args.impl == "reference":
-            print(json.dumps({"impl": "reference", "unavailable": "the refgpu workload is itself a comparison"}))
-            return
-        run_refgpu(args)
-        return
-    if args.workload in ("batch", "serve"):
-        if args.impl == "reference":
-            if int(os.environ.get("RANK", "0")) == 0:
-                print(json.dumps({"impl": "reference",
-                                  "unavailable": f"the {args.workload} workload has no reference path"}))
-            return
-        run_batch(args) if args.workload == "batch" else run_serve(args)
-    elif args.impl == "reference":
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "refgpu":
+        run_refgpu(args)
+    elif args.workload == "batch" and world > 1:
+        run_batch_multi(args)
+    elif args.workload in ("grid", "batch", "serve"):
+        if int(os.environ.get("RANK", "0")) == 0:
+            run_workload(args)
     else:
         run_ours(args)
 

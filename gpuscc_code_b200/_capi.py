@@ -86,7 +86,8 @@ class scc_request_info(C.Structure):
 
 class scc_server_stats(C.Structure):
     _fields_ = [(k, C.c_uint64) for k in ("submitted", "completed", "rejected", "batches", "graphs_batched",
-                                           "resident_bytes", "peak_resident_bytes", "budget_bytes")]
+                                           "resident_bytes", "peak_resident_bytes", "budget_bytes",
+                                           "registered", "evictions", "reuploads")]
 
     def as_dict(self) -> dict:
         return {name: int(getattr(self, name)) for name, _ in self._fields_}
@@ -166,6 +167,9 @@ SIGNATURES = [
     ("scc_server_start", C.c_int, [C.POINTER(scc_server_cfg), C.POINTER(C.c_void_p)]),
     ("scc_server_set_model", C.c_int, [C.c_void_p, f32p, f32p, f32p]),
     ("scc_server_submit", C.c_int, [C.c_void_p, C.POINTER(scc_host_csr), u32p, C.POINTER(C.c_uint64)]),
+    ("scc_server_register", C.c_int, [C.c_void_p, C.POINTER(scc_host_csr), C.POINTER(C.c_uint64)]),
+    ("scc_server_submit_resident", C.c_int, [C.c_void_p, C.c_uint64, u32p, C.POINTER(C.c_uint64)]),
+    ("scc_server_unregister", C.c_int, [C.c_void_p, C.c_uint64]),
     ("scc_server_poll", C.c_int, [C.c_void_p, C.c_uint64, C.POINTER(scc_request_info)]),
     ("scc_server_wait", C.c_int, [C.c_void_p, C.c_uint64, C.c_uint32, C.POINTER(scc_request_info)]),
     ("scc_server_get_stats", C.c_int, [C.c_void_p, C.POINTER(scc_server_stats)]),

@@ -72,7 +72,7 @@ struct scc_ctx {
   // per-vertex state
   uint32_t cap_n = 0, cap_h = 0;
   bool have_state = false;
-  DBuf label, range, rpivot, aux, bitmaps, qa, qb, act0, act1, piv, pivkey, slot, heavy, ctl, seg;
+  DBuf label, range, rpivot, aux, sccsize, bitmaps, qa, qb, act0, act1, piv, pivkey, slot, heavy, ctl, seg;
   DBuf feat;  // scratch of scc_graph_features
   uint32_t nwords = 0;
   bool slot_dirty = true;
@@ -104,6 +104,10 @@ int use_device(scc_ctx *c) {
   return SCC_OK;
 }
 
+}  // namespace
+
+namespace sccb {
+
 int check_opts(const scc_opts *o) {
   if (o->alg < SCC_ALG_QUADRATIC || o->alg > SCC_ALG_BEST) return set_error(SCC_ERR_INVALID, "unknown alg %d", o->alg);
   if (o->block_size != 0 && o->block_size != 128 && o->block_size != 256 && o->block_size != 512 &&
@@ -118,6 +122,12 @@ int check_opts(const scc_opts *o) {
   return SCC_OK;
 }
 
+}  // namespace sccb
+
+namespace {
+
+using sccb::check_opts;
+
 int ensure_state(scc_ctx *c) {
   const uint32_t n = c->n;
   const uint32_t hcap = c->m / 256u + 2u;
@@ -130,6 +140,7 @@ int ensure_state(scc_ctx *c) {
   CK(c->range.ensure(vb), "alloc ranges");
   CK(c->rpivot.ensure(vb), "alloc pivots");
   CK(c->aux.ensure(vb), "alloc aux");
+  CK(c->sccsize.ensure(vb), "alloc component sizes");
   CK(c->bitmaps.ensure((size_t)nw * 4 * 7), "alloc bitmaps");
   CK(c->qa.ensure(vb), "alloc queue");
   CK(c->qb.ensure(vb), "alloc queue");
@@ -167,6 +178,7 @@ sccb::Params make_params(scc_ctx *c, uint32_t *out_labels) {
   s.range = c->range.as<uint32_t>();
   s.rpivot = c->rpivot.as<uint32_t>();
   s.aux = c->aux.as<uint32_t>();
+  s.sccsize = c->sccsize.as<uint32_t>();
   // bitmaps sized for this graph (words beyond it are never touched)
   const uint32_t nw = sccb::bitmap_words(c->n);
   uint32_t *bm = c->bitmaps.as<uint32_t>();
@@ -281,6 +293,11 @@ void fill_stats(scc_ctx *c, scc_stats *st, float ms) {
   st->n_trim2 = k.n_trim2;
   st->n_fb_elim = k.n_fbe + k.n_trim2;
   st->nscc = k.nscc;
+  // trim-1 removes singletons, trim-2 pairs; F∩B components were counted per pivot
+  uint32_t largest = k.largest_fb;
+  if (k.n_trim2 && largest < 2u) largest = 2u;
+  if (k.n_trimmed && largest < 1u) largest = 1u;
+  st->largest_scc = largest;
   st->pull_sweeps = k.pull_sweeps;
   st->grid_blocks = c->grid_used;
   st->block_size = (uint32_t)block_size_of(c);
@@ -353,7 +370,7 @@ int scc_ctx_destroy(scc_ctx *c) {
   if (!c) return SCC_OK;
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
-  for (DBuf *b : {&c->g_off, &c->g_adj, &c->g_offT, &c->g_adjT, &c->label, &c->range, &c->rpivot, &c->aux,
+  for (DBuf *b : {&c->g_off, &c->g_adj, &c->g_offT, &c->g_adjT, &c->label, &c->range, &c->rpivot, &c->aux, &c->sccsize,
                   &c->bitmaps, &c->qa, &c->qb, &c->act0, &c->act1, &c->piv, &c->pivkey, &c->slot, &c->heavy,
                   &c->ctl, &c->seg, &c->feat})
     b->release();

@@ -36,6 +36,7 @@ constexpr uint32_t kLocalMax = 2048, kLocalEdges = 4096, kLocalLevels = 4096;
 enum : uint32_t { ARM_Q = 0, ARM_T = 1, ARM_D = 2, ARM_L = 3, ARM_B = 6 };
 
 constexpr int kSlotCache = 128;  // per-CTA cache of partition-election slots
+constexpr int kSizeCache = 32;   // per-CTA cache of SCC-size counters
 
 template <int BS>
 struct Eng {
@@ -109,6 +110,23 @@ struct Eng {
   __device__ void add_count(uint32_t *dst, uint32_t x) {
     const uint32_t s = block_sum(x);
     if (threadIdx.x == 0 && s) atomicAdd(dst, s);
+  }
+
+  // Members of the SCC of pivot p eliminated together: a CTA-local cache
+  // (kSizeCache direct-mapped slots) absorbs the adds of its few large
+  // components, so a giant SCC costs one global atomic per CTA, not one per
+  // warp.  Running totals only grow, so the largest total any add returns
+  // is the largest component.
+  __device__ void size_flush(uint32_t p, uint32_t cnt) {
+    const uint32_t tot = atomicAdd(P.s.sccsize + p, cnt) + cnt;
+    if (tot > ldm(&c->largest_fb)) atomicMax(&c->largest_fb, tot);
+  }
+  __device__ void size_add(uint32_t *s_szkey, uint32_t *s_szcnt, uint32_t p, uint32_t cnt) {
+    const uint32_t h = p % kSizeCache;
+    uint32_t owner = s_szkey[h];
+    if (owner == kNone) owner = atomicCAS(&s_szkey[h], kNone, p) == kNone ? p : s_szkey[h];
+    if (owner == p) atomicAdd(&s_szcnt[h], cnt);
+    else size_flush(p, cnt);
   }
 
   __device__ uint32_t gtid() const { return blockIdx.x * BS + threadIdx.x; }
@@ -564,6 +582,7 @@ struct Eng {
     if (is_lead()) {
       if (p) {
         P.s.rpivot[0] = p;
+        P.s.sccsize[p] = 0u;
         P.s.piv[0] = p;
         bit_set(P.s.fvis, p);
         bit_set(P.s.bvis, p);
@@ -584,9 +603,14 @@ struct Eng {
     const EngState &s = P.s;
     __shared__ uint32_t s_key[kSlotCache];
     __shared__ unsigned long long s_val[kSlotCache];
+    __shared__ uint32_t s_szkey[kSizeCache], s_szcnt[kSizeCache];
     for (int i = threadIdx.x; i < kSlotCache; i += BS) {
       s_key[i] = kNone;
       s_val[i] = ~0ull;
+    }
+    for (int i = threadIdx.x; i < kSizeCache; i += BS) {
+      s_szkey[i] = kNone;
+      s_szcnt[i] = 0u;
     }
     __syncthreads();
     uint32_t nelim = 0, nfound = 0;
@@ -611,10 +635,11 @@ struct Eng {
       uint32_t key = kNone;
       unsigned long long val = ~0ull;
       bool fb = false;
+      uint32_t p = kNone;
       if (valid && !((ew >> (v & 31u)) & 1u)) {
         const bool f = (fw >> (v & 31u)) & 1u, b = (bw >> (v & 31u)) & 1u;
         if (f && b) {
-          const uint32_t p = r ? r : p0;
+          p = r ? r : p0;
           s.label[v] = p;
           fb = true;
           ++nelim;
@@ -625,6 +650,10 @@ struct Eng {
         }
       }
       warp_set_bits(s.elim, v, fb, !list_mode);
+      {  // SCC sizes: the warp's members of one component counted together
+        const uint32_t pg = __match_any_sync(kFull, p);
+        if (fb && lane_id() == (uint32_t)(__ffs(pg) - 1)) size_add(s_szkey, s_szcnt, p, __popc(pg));
+      }
       const uint32_t grp = __match_any_sync(kFull, key);
       if (key != kNone) {
         const uint32_t hi = (uint32_t)(val >> 32), lo = (uint32_t)val;
@@ -648,6 +677,8 @@ struct Eng {
       const uint32_t key = s_key[i];
       if (key != kNone && ldm64(s.slot + key) > s_val[i]) atomicMin(s.slot + key, s_val[i]);
     }
+    for (int i = threadIdx.x; i < kSizeCache; i += BS)
+      if (s_szkey[i] != kNone) size_flush(s_szkey[i], s_szcnt[i]);
     add_count(&c->n_fbe, nelim);
     add_count(&c->n_fbscc, nfound);
     if (!bar(300)) return;
@@ -706,6 +737,7 @@ struct Eng {
       if (valid) {
         const uint32_t p = ldm(s.piv + i);
         s.rpivot[p] = p;
+        s.sccsize[p] = 0u;
         bit_set(s.fvis, p);
         bit_set(s.bvis, p);
       }
@@ -1417,7 +1449,10 @@ struct Eng {
         const uint32_t r = ldm(lab + v);
         s.range[v] = r;
         root = r == v;
-        if (root) s.rpivot[v] = v;
+        if (root) {
+          s.rpivot[v] = v;
+          s.sccsize[v] = 0u;
+        }
       }
       warp_push(s.piv, cur() + C_Q, s.qcap, v, root, err());
     });

@@ -35,7 +35,7 @@ struct Ctl {
   uint32_t wcc_done;
   uint32_t phase_ret, phase_ret2;
   uint32_t trim_first_done;
-  uint32_t pad0;
+  uint32_t largest_fb;          // largest SCC found as F∩B (members counted per pivot)
   unsigned long long ns_trim, ns_fwd, ns_bwd, ns_update, ns_wcc;
   // finer device timers (globaltimer, CTA 0) and counts, indexed by Prof
   unsigned long long prof_ns[16];
@@ -76,6 +76,7 @@ struct EngState {
   uint32_t *range;   // n+1: partition id (the pivot id of the partition after the first selection)
   uint32_t *rpivot;  // n+1: pivot of partition id
   uint32_t *aux;     // n+1: WCC colours / trim-2 partners / canonical ids
+  uint32_t *sccsize; // n+1: F∩B members counted per pivot (zeroed when the pivot is elected)
   uint32_t *elim, *fvis, *bvis, *fexp, *bexp, *tflag, *queued;  // bitmaps, nwords each
   uint32_t *qa, *qb;       // queues, qcap each
   uint32_t *act[2];        // active lists, qcap each

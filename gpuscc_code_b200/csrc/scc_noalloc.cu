@@ -1,23 +1,28 @@
 // scc_solve_noalloc: the whole decomposition without any device allocation.
 //
-// Some callers cannot call cudaMalloc: code that runs while a CUDA stream is
-// being captured into a graph (allocation is not a capturable operation),
-// plugins hosted by a framework that owns the whole device-memory budget and
-// forbids side allocations, and latency-critical host loops that must not hit
-// the allocator's implicit device synchronisation.  For them this entry point
-// runs the same persistent solve kernel as scc_solve_device, with every
-// scratch buffer (labels, partitions, bitmaps, worklists, election slots,
+// Some callers cannot call cudaMalloc: plugins hosted by a framework that
+// owns the whole device-memory budget and forbids side allocations (the
+// framework's allocator, not the plugin, decides what lives on the device),
+// and latency-critical host loops that must not hit the allocator's implicit
+// device synchronisation.  For them this entry point runs the same
+// persistent solve kernel as scc_solve_device, with every scratch buffer
+// (labels, partitions, component sizes, bitmaps, worklists, election slots,
 // control block) carved out of one file-scope device array instead of
 // context-owned allocations.  The caller still passes the graph and the
-// label output as device pointers.
+// label output as device pointers.  The call returns once the solve has
+// finished: it waits for `stream` to read back the result.
 //
 // Limits: at most kMaxN vertices and kMaxM edges per graph (the array is
-// about 4.7 MB; every GPU that loads this library holds it until the process
-// exits).  All calls share the array: calls that overlap on the GPU (two
+// about 5 MB; every GPU that loads this library holds it until the process
+// exits).  All calls share the array and it keeps the last call's contents;
+// each call resets what must start fresh.  Calls that overlap on the GPU (two
 // streams, two host threads) race on it and must be serialised by the caller.
 // The first call on a device performs a one-time set-up for that device
 // (looking up the array's device address with cudaGetSymbolAddress while the
-// device is current); make that first call before any stream capture.
+// device is current).  cudaDeviceReset unloads the module that holds the
+// array, so the address found by the set-up is no longer valid afterwards:
+// a process that resets a device must not call this entry point on that
+// device again (scc_solve_device has no such restriction).
 #include <cuda_runtime.h>
 
 #include <cstring>
@@ -40,7 +45,7 @@ constexpr uint32_t kHeavyCap = kMaxM / 256u + 2u;
 constexpr size_t kHeavy = a256(size_t(kHeavyCap) * 5 * 4);
 constexpr size_t kCtl = a256(sizeof(sccb::Ctl));
 constexpr size_t kFlag = 256;  // CSR check flag
-constexpr size_t kScratchBytes = 10 * kVec + kBitmaps + kSlots + kHeavy + kCtl + kFlag;
+constexpr size_t kScratchBytes = 11 * kVec + kBitmaps + kSlots + kHeavy + kCtl + kFlag;
 
 }  // namespace
 
@@ -87,13 +92,14 @@ extern "C" int scc_solve_noalloc(const scc_dev_csr *g, const scc_opts *opts, uin
   scc_opts o;
   scc_opts_default(&o);
   if (opts) o = *opts;
-  if (o.alg < SCC_ALG_QUADRATIC || o.alg > SCC_ALG_BEST || o.pivot_rule < 0 || o.pivot_rule > 1 ||
-      (o.block_size != 0 && o.block_size != 128 && o.block_size != 256 && o.block_size != 512 &&
-       o.block_size != 1024) ||
-      o.switch_permille < 0 || o.switch_permille > 1000 || (o.heavy_degree != 0 && o.heavy_degree < 256))
-    return sccb::set_error(SCC_ERR_INVALID, "invalid options");
+  int rc = sccb::check_opts(&o);  // the same option set as the context entry points
+  if (rc) return rc;
+  // an error left by the caller's earlier work would otherwise surface as this solve's
+  cudaError_t pending = cudaGetLastError();
+  if (pending != cudaSuccess)
+    return sccb::set_error(SCC_ERR_CUDA, "pending CUDA error before the solve: %s", cudaGetErrorString(pending));
   unsigned char *base = nullptr;
-  int rc = scratch_for_current_device(&base);
+  rc = scratch_for_current_device(&base);
   if (rc) return rc;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   const uint32_t n = g->n;
@@ -118,6 +124,7 @@ extern "C" int scc_solve_noalloc(const scc_dev_csr *g, const scc_opts *opts, uin
   s.range = vec();
   s.rpivot = vec();
   s.aux = vec();
+  s.sccsize = vec();
   s.qa = vec();
   s.qb = vec();
   s.act[0] = vec();

@@ -1,22 +1,26 @@
 // Request loop with continuous batching on one device.
 //
 // Three parties share the request table under one mutex:
-//  * callers: scc_server_submit appends a request (rejected at once when its
-//    CSR alone exceeds the memory budget) and poll/wait read its result;
-//  * the admission thread takes requests in arrival order, waits until the
-//    resident bytes plus the request's CSR fit the budget, allocates the CSR
-//    from the stream-ordered pool and uploads it on the copy stream while
-//    the solver is busy with earlier batches;
-//  * the solver thread, whenever the device is free, takes every uploaded
+//  * callers: scc_server_register uploads a graph once and keeps its CSR
+//    resident under a handle; scc_server_submit_resident queues a solve of a
+//    resident graph (no upload), scc_server_submit one of a host graph
+//    (uploaded for that request only); poll/wait read the result;
+//  * the admission thread takes the requests that need an upload in arrival
+//    order (host graphs, and resident graphs whose device copy was evicted),
+//    waits until the resident bytes plus the upload fit the budget -- evicting
+//    resident graphs that no request uses, least recently used first --
+//    allocates from the stream-ordered pool and uploads on the copy stream
+//    while the solver is busy with earlier batches;
+//  * the solver thread, whenever the device is free, takes every ready
 //    request (oldest first) whose options match the oldest one's, up to the
 //    batch limits, packs them into one segmented CSR with a device kernel (a
 //    single graph is bound in place), runs one persistent solve, unpacks each
 //    segment's labels back to local ids and copies them to the caller's
-//    buffer, then frees the request's device memory.
-// With a strategy network loaded, the admission thread also launches each
-// request's feature pass on a stream of its own (behind the upload, never in
-// front of the next one); the solver reads the features when it forms a
-// batch and lets the network pick the options of all new requests at once.
+//    buffer, then frees a host graph's device copy (a resident one stays).
+// With a strategy network loaded, each uploaded graph's feature pass runs on
+// a stream of its own (behind the upload, never in front of the next one);
+// the solver reads the features when it forms a batch and lets the network
+// pick the options of all new requests at once (once per resident graph).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -82,27 +86,51 @@ __global__ void unpack_kernel(const PackDesc *__restrict__ d, uint32_t *labels, 
 
 enum ReqState { RQ_QUEUED, RQ_UPLOADING, RQ_READY, RQ_RUNNING, RQ_DONE };
 
-struct Request {
-  uint64_t id = 0;
+uint64_t pad4(uint64_t x) { return (x + 3) & ~uint64_t(3); }
+
+// A graph's device copy: one allocation off | offT | adj | adjT, its upload
+// event and, with a network loaded, its feature pass.
+struct DevGraph {
   scc_host_csr g{};
-  uint32_t *labels = nullptr;
   uint64_t bytes = 0;
-  ReqState state = RQ_QUEUED;
-  Clock::time_point t_submit, t_admit, t_done;
-  void *dmem = nullptr;  // one allocation: off | offT | adj | adjT
+  void *dmem = nullptr;
   cudaEvent_t uploaded = nullptr;
-  bool have_choice = false;
-  int32_t choice[3] = {0, 0, 0};
   void *h_acc = nullptr;  // page-locked slot receiving the feature accumulators
   bool feat_pending = false;
-  cudaEvent_t featured = nullptr;  // features of this request done (feature stream)
-  scc_request_info info{};
+  cudaEvent_t featured = nullptr;  // features done (feature stream)
+  bool have_choice = false;
+  int32_t choice[3] = {0, 0, 0};
   const uint32_t *d_off() const { return static_cast<const uint32_t *>(dmem); }
   const uint32_t *d_offT() const { return d_off() + pad4(g.n + 2); }
   const uint32_t *d_adj() const { return d_offT() + pad4(g.n + 2); }
   const uint32_t *d_adjT() const { return d_adj() + pad4(g.m); }
-  static uint64_t pad4(uint64_t x) { return (x + 3) & ~uint64_t(3); }
   static uint64_t csr_bytes(uint32_t n, uint32_t m) { return (2 * pad4(n + 2) + 2 * pad4(m)) * 4; }
+};
+
+// A registered graph: the caller's host arrays (valid until unregistered)
+// and, while resident, its device copy.  pending counts the requests that
+// name it and are not finished; only a graph with none may be evicted.
+struct Resident {
+  uint64_t handle = 0;
+  DevGraph dg;
+  uint32_t pending = 0;
+  uint64_t last_use = 0;         // LRU clock of the last request
+  bool uploading = false;
+  cudaEvent_t released = nullptr;  // solve-stream point after the last finished request
+};
+
+struct Request {
+  uint64_t id = 0;
+  DevGraph own;              // a host graph's per-request copy
+  Resident *res = nullptr;   // or the resident graph it names
+  uint32_t *labels = nullptr;
+  ReqState state = RQ_QUEUED;
+  Clock::time_point t_submit, t_admit, t_done;
+  bool have_choice = false;
+  int32_t choice[3] = {0, 0, 0};
+  scc_request_info info{};
+  DevGraph &dev() { return res ? res->dg : own; }
+  const scc_host_csr &g() { return dev().g; }
 };
 
 double ms_between(Clock::time_point a, Clock::time_point b) {
@@ -129,7 +157,8 @@ struct scc_server {
   std::condition_variable cv_admit, cv_solve, cv_done;
   std::deque<Request *> admit_q;
   std::map<uint64_t, std::unique_ptr<Request>> reqs;
-  uint64_t next_id = 1;
+  std::map<uint64_t, std::unique_ptr<Resident>> residents;
+  uint64_t next_id = 1, next_handle = 1, lru_clock = 0;
   bool stopping = false;
   scc_server_stats st{};
   std::thread admit_thr, solve_thr;
@@ -138,6 +167,11 @@ struct scc_server {
   void solve_loop();
   int run_batch(std::vector<Request *> &batch);
   int choose(std::vector<Request *> &ready);
+  cudaError_t upload(DevGraph &d);
+  cudaError_t start_features(DevGraph &d);
+  bool make_room(uint64_t bytes);
+  void evict(Resident *r);
+  void release_dev(DevGraph &d, cudaStream_t order);
   // page-locked slots for feature accumulators (one per request in flight)
   std::mutex acc_mu;
   std::vector<void *> acc_free, acc_chunks;
@@ -160,67 +194,140 @@ int srv_fail(cudaError_t e, const char *what) {
 
 }  // namespace
 
+// Pool allocation + upload of d's host arrays on the copy stream; with a
+// network loaded, the graph's feature pass follows on its own stream.
+// Called without the lock; d.dmem is published by the caller.
+cudaError_t scc_server::upload(DevGraph &d) {
+  void *mem = nullptr;
+  cudaError_t e = cudaMallocFromPoolAsync(&mem, d.bytes, pool, copy_st);
+  if (e != cudaSuccess) return e;
+  d.dmem = mem;
+  const size_t nb = ((size_t)d.g.n + 2) * 4, mb = (size_t)d.g.m * 4;
+  e = cudaMemcpyAsync(const_cast<uint32_t *>(d.d_off()), d.g.nodes, nb, cudaMemcpyHostToDevice, copy_st);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(const_cast<uint32_t *>(d.d_offT()), d.g.nodesT, nb, cudaMemcpyHostToDevice, copy_st);
+  if (e == cudaSuccess && mb)
+    e = cudaMemcpyAsync(const_cast<uint32_t *>(d.d_adj()), d.g.edges, mb, cudaMemcpyHostToDevice, copy_st);
+  if (e == cudaSuccess && mb)
+    e = cudaMemcpyAsync(const_cast<uint32_t *>(d.d_adjT()), d.g.edgesT, mb, cudaMemcpyHostToDevice, copy_st);
+  if (e == cudaSuccess && !d.uploaded) e = cudaEventCreateWithFlags(&d.uploaded, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventRecord(d.uploaded, copy_st);
+  // the features are computed behind the upload with nothing waiting for them
+  // (the next uploads go on): the solver reads the accumulators when it forms
+  // the batch that takes the graph
+  if (e == cudaSuccess && mlp && !d.feat_pending) e = start_features(d);
+  return e;
+}
+
+cudaError_t scc_server::start_features(DevGraph &d) {
+  void *scratch = nullptr;
+  const size_t fb = sccb::features_scratch_bytes(d.g.n);
+  if (!d.h_acc) d.h_acc = get_acc();
+  cudaError_t e = d.h_acc ? cudaStreamWaitEvent(feat_st, d.uploaded, 0) : cudaErrorMemoryAllocation;
+  if (e == cudaSuccess) e = cudaMallocFromPoolAsync(&scratch, fb, pool, feat_st);
+  if (e != cudaSuccess) return e;
+  sccb::EngGraph g{};
+  g.n = d.g.n;
+  g.m = d.g.m;
+  g.sorted_unique = d.g.sorted_unique ? 1u : 0u;
+  g.off = d.d_off();
+  g.adj = d.d_adj();
+  g.offT = d.d_offT();
+  g.adjT = d.d_adjT();
+  e = sccb::graph_features_launch(g, scratch, fb, d.h_acc, feat_st);
+  cudaFreeAsync(scratch, feat_st);
+  if (e == cudaSuccess && !d.featured) e = cudaEventCreateWithFlags(&d.featured, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventRecord(d.featured, feat_st);
+  d.feat_pending = e == cudaSuccess;
+  return e;
+}
+
+// Frees d's device copy in stream order: after `order`'s pending work (the
+// solve stream, or the copy stream behind a recorded release point), after
+// the upload and the feature pass that read it.
+void scc_server::release_dev(DevGraph &d, cudaStream_t order) {
+  if (d.uploaded) cudaStreamWaitEvent(order, d.uploaded, 0);
+  if (d.featured) cudaStreamWaitEvent(order, d.featured, 0);
+  if (d.h_acc) {
+    if (d.featured) cudaEventSynchronize(d.featured);  // the accumulator copy lands in the slot
+    put_acc(d.h_acc);
+    d.h_acc = nullptr;
+  }
+  d.feat_pending = false;
+  if (d.dmem) cudaFreeAsync(d.dmem, order);
+  d.dmem = nullptr;
+}
+
+// Evicts resident graph r (lock held; no request names it).
+void scc_server::evict(Resident *r) {
+  if (r->released) cudaStreamWaitEvent(copy_st, r->released, 0);
+  release_dev(r->dg, copy_st);
+  st.resident_bytes -= r->dg.bytes;
+  ++st.evictions;
+}
+
+// Makes `bytes` fit the budget by evicting resident graphs that no request
+// names, least recently used first (lock held).  False, evicting nothing,
+// when even all of those would not free enough.
+bool scc_server::make_room(uint64_t bytes) {
+  if (st.resident_bytes + bytes <= st.budget_bytes) return true;
+  uint64_t evictable = 0;
+  for (auto &kv : residents) {
+    const Resident *r = kv.second.get();
+    if (!r->uploading && !r->pending && r->dg.dmem) evictable += r->dg.bytes;
+  }
+  if (st.resident_bytes - evictable + bytes > st.budget_bytes) return false;
+  while (st.resident_bytes + bytes > st.budget_bytes) {
+    Resident *victim = nullptr;
+    for (auto &kv : residents) {
+      Resident *r = kv.second.get();
+      if (!r->uploading && !r->pending && r->dg.dmem && (!victim || r->last_use < victim->last_use)) victim = r;
+    }
+    evict(victim);
+  }
+  return true;
+}
+
 void scc_server::admit_loop() {
   cudaSetDevice(cfg.device);
   std::unique_lock<std::mutex> lk(mu);
   for (;;) {
     cv_admit.wait(lk, [&] {
       if (admit_q.empty()) return stopping;
-      return st.resident_bytes + admit_q.front()->bytes <= st.budget_bytes;
+      Request *r = admit_q.front();
+      if (r->res) return !r->res->uploading && (r->res->dg.dmem != nullptr || make_room(r->res->dg.bytes));
+      return make_room(r->own.bytes);
     });
     if (admit_q.empty()) return;  // stopping and drained
     Request *r = admit_q.front();
     admit_q.pop_front();
-    st.resident_bytes += r->bytes;
+    r->t_admit = Clock::now();
+    if (r->res && r->res->dg.dmem) {  // uploaded meanwhile (another request of the same graph, or register)
+      r->state = RQ_READY;
+      cv_solve.notify_one();
+      continue;
+    }
+    DevGraph &d = r->dev();
+    if (r->res) {
+      r->res->uploading = true;
+      ++st.reuploads;
+    }
+    st.resident_bytes += d.bytes;
     st.peak_resident_bytes = std::max(st.peak_resident_bytes, st.resident_bytes);
     r->state = RQ_UPLOADING;
-    r->t_admit = Clock::now();
     lk.unlock();
-    cudaError_t e = cudaMallocFromPoolAsync(&r->dmem, r->bytes, pool, copy_st);
-    if (e == cudaSuccess) {
-      uint32_t *o = const_cast<uint32_t *>(r->d_off());
-      const size_t nb = ((size_t)r->g.n + 2) * 4, mb = (size_t)r->g.m * 4;
-      e = cudaMemcpyAsync(o, r->g.nodes, nb, cudaMemcpyHostToDevice, copy_st);
-      if (e == cudaSuccess)
-        e = cudaMemcpyAsync(const_cast<uint32_t *>(r->d_offT()), r->g.nodesT, nb, cudaMemcpyHostToDevice, copy_st);
-      if (e == cudaSuccess && mb)
-        e = cudaMemcpyAsync(const_cast<uint32_t *>(r->d_adj()), r->g.edges, mb, cudaMemcpyHostToDevice, copy_st);
-      if (e == cudaSuccess && mb)
-        e = cudaMemcpyAsync(const_cast<uint32_t *>(r->d_adjT()), r->g.edgesT, mb, cudaMemcpyHostToDevice, copy_st);
-      if (e == cudaSuccess) e = cudaEventCreateWithFlags(&r->uploaded, cudaEventDisableTiming);
-      if (e == cudaSuccess) e = cudaEventRecord(r->uploaded, copy_st);
-      // with a network loaded, the graph's features are computed on their own
-      // stream behind the upload, with nothing waiting for them (the next
-      // uploads go on): the solver reads the accumulators when it forms the
-      // batch that may take r
-      if (e == cudaSuccess && mlp) {
-        void *scratch = nullptr;
-        const size_t fb = sccb::features_scratch_bytes(r->g.n);
-        r->h_acc = get_acc();
-        e = r->h_acc ? cudaStreamWaitEvent(feat_st, r->uploaded, 0) : cudaErrorMemoryAllocation;
-        if (e == cudaSuccess) e = cudaMallocFromPoolAsync(&scratch, fb, pool, feat_st);
-        if (e == cudaSuccess) {
-          sccb::EngGraph g{};
-          g.n = r->g.n;
-          g.m = r->g.m;
-          g.sorted_unique = r->g.sorted_unique ? 1u : 0u;
-          g.off = r->d_off();
-          g.adj = r->d_adj();
-          g.offT = r->d_offT();
-          g.adjT = r->d_adjT();
-          e = sccb::graph_features_launch(g, scratch, fb, r->h_acc, feat_st);
-          cudaFreeAsync(scratch, feat_st);
-          if (e == cudaSuccess) e = cudaEventCreateWithFlags(&r->featured, cudaEventDisableTiming);
-          if (e == cudaSuccess) e = cudaEventRecord(r->featured, feat_st);
-          r->feat_pending = e == cudaSuccess;
-        }
-      }
-    }
+    const cudaError_t e = upload(d);
     lk.lock();
+    if (r->res) {
+      r->res->uploading = false;
+      cv_admit.notify_all();
+    }
     if (e != cudaSuccess) {
       sccb::set_error(SCC_ERR_CUDA, "upload: %s", cudaGetErrorString(e));
       cudaStreamSynchronize(copy_st);  // nothing may still write into the allocation when it is freed
       cudaStreamSynchronize(feat_st);
+      release_dev(d, copy_st);
+      if (r->res) st.resident_bytes -= d.bytes;  // a host graph's bytes are returned by finish
       lk.unlock();
       finish(r, e == cudaErrorMemoryAllocation ? SCC_ERR_NOMEM : SCC_ERR_CUDA);
       lk.lock();
@@ -231,24 +338,25 @@ void scc_server::admit_loop() {
   }
 }
 
-// Marks r done with the given status, releases its device memory (ordered
-// after the solve stream's work) and wakes waiters.
+// Marks r done with the given status, releases a host graph's device copy
+// (ordered after the solve stream's work; a resident graph keeps its copy and
+// records where the solve stream stopped using it) and wakes waiters.
 void scc_server::finish(Request *r, int status) {
-  if (r->uploaded) cudaStreamWaitEvent(solve_st, r->uploaded, 0);  // the upload may still be in flight
-  if (r->featured) cudaStreamWaitEvent(solve_st, r->featured, 0);  // and the feature pass reading the graph
-  if (r->h_acc) {
-    if (r->featured) cudaEventSynchronize(r->featured);  // the accumulator copy lands in the slot
-    put_acc(r->h_acc);
-    r->h_acc = nullptr;
+  if (!r->res) {
+    release_dev(r->own, solve_st);
+    if (r->own.uploaded) cudaEventDestroy(r->own.uploaded);
+    if (r->own.featured) cudaEventDestroy(r->own.featured);
+    r->own.uploaded = r->own.featured = nullptr;
   }
-  if (r->featured) cudaEventDestroy(r->featured);
-  r->featured = nullptr;
-  if (r->dmem) cudaFreeAsync(r->dmem, solve_st);
-  r->dmem = nullptr;
-  if (r->uploaded) cudaEventDestroy(r->uploaded);
-  r->uploaded = nullptr;
   std::lock_guard<std::mutex> lk(mu);
-  st.resident_bytes -= r->bytes;
+  if (r->res) {
+    Resident *res = r->res;
+    if (!res->released) cudaEventCreateWithFlags(&res->released, cudaEventDisableTiming);
+    if (res->released) cudaEventRecord(res->released, solve_st);
+    --res->pending;
+  } else if (r->state != RQ_QUEUED) {
+    st.resident_bytes -= r->own.bytes;
+  }
   r->t_done = Clock::now();
   r->info.status = status;
   r->info.queue_ms = ms_between(r->t_submit, r->t_admit);
@@ -282,32 +390,48 @@ void scc_server::put_acc(void *p) {
 }
 
 // Choices for the ready requests that have none: their features were
-// launched at admission; one forward pass of the network covers them all.
-// Without a network (or without features) a request keeps choice (0,0,0),
-// the plain method.
+// launched at upload (or, for a resident graph uploaded before the network
+// was loaded, are launched now); one forward pass of the network covers all
+// of them, and a resident graph keeps its choice for its later requests.
+// Without a network a request keeps choice (0,0,0), the plain method.
 int scc_server::choose(std::vector<Request *> &ready) {
-  std::vector<Request *> todo;
+  std::vector<DevGraph *> todo;
   for (Request *r : ready) {
     if (r->have_choice) continue;
-    if (!mlp || !r->feat_pending) {
+    DevGraph &d = r->dev();
+    if (!mlp || d.have_choice) {
+      if (mlp) std::memcpy(r->choice, d.choice, sizeof(r->choice));
       r->have_choice = true;
       continue;
     }
-    todo.push_back(r);
+    if (!d.feat_pending) {
+      cudaError_t e = start_features(d);
+      if (e != cudaSuccess) {  // the plain method stays the fallback
+        r->have_choice = true;
+        continue;
+      }
+    }
+    if (std::find(todo.begin(), todo.end(), &d) == todo.end()) todo.push_back(&d);
   }
-  if (todo.empty()) return SCC_OK;
-  std::vector<float> x(todo.size() * sccb::kFeatures);
-  for (size_t i = 0; i < todo.size(); ++i) {
-    Request *r = todo[i];
-    SCK(cudaEventSynchronize(r->featured), "features");
-    sccb::graph_features_finish(r->g.n, r->g.m, r->h_acc, &x[i * sccb::kFeatures]);
+  if (!todo.empty()) {
+    std::vector<float> x(todo.size() * sccb::kFeatures);
+    for (size_t i = 0; i < todo.size(); ++i) {
+      DevGraph *d = todo[i];
+      SCK(cudaEventSynchronize(d->featured), "features");
+      sccb::graph_features_finish(d->g.n, d->g.m, d->h_acc, &x[i * sccb::kFeatures]);
+    }
+    std::vector<int32_t> ch(todo.size() * 3);
+    int rc = scc_mlp_predict(mlp, x.data(), (uint32_t)todo.size(), ch.data());
+    if (rc) return rc;
+    for (size_t i = 0; i < todo.size(); ++i) {
+      std::memcpy(todo[i]->choice, &ch[i * 3], sizeof(todo[i]->choice));
+      todo[i]->have_choice = true;
+    }
   }
-  std::vector<int32_t> ch(todo.size() * 3);
-  int rc = scc_mlp_predict(mlp, x.data(), (uint32_t)todo.size(), ch.data());
-  if (rc) return rc;
-  for (size_t i = 0; i < todo.size(); ++i) {
-    std::memcpy(todo[i]->choice, &ch[i * 3], sizeof(todo[i]->choice));
-    todo[i]->have_choice = true;
+  for (Request *r : ready) {
+    if (r->have_choice) continue;
+    std::memcpy(r->choice, r->dev().choice, sizeof(r->choice));
+    r->have_choice = true;
   }
   return SCC_OK;
 }
@@ -320,14 +444,14 @@ int scc_server::run_batch(std::vector<Request *> &batch) {
   }
   int rc = scc_ctx_set_opts(ctx, &o);
   if (rc) return rc;
-  for (Request *r : batch) SCK(cudaStreamWaitEvent(solve_st, r->uploaded, 0), "wait upload");
+  for (Request *r : batch) SCK(cudaStreamWaitEvent(solve_st, r->dev().uploaded, 0), "wait upload");
   uint64_t N = 0, M = 0;
   std::vector<PackDesc> desc(batch.size());
   for (size_t i = 0; i < batch.size(); ++i) {
-    Request *r = batch[i];
-    desc[i] = PackDesc{r->d_off(), r->d_adj(), r->d_offT(), r->d_adjT(), r->g.n, r->g.m, (uint32_t)N, (uint32_t)M};
-    N += r->g.n;
-    M += r->g.m;
+    const DevGraph &d = batch[i]->dev();
+    desc[i] = PackDesc{d.d_off(), d.d_adj(), d.d_offT(), d.d_adjT(), d.g.n, d.g.m, (uint32_t)N, (uint32_t)M};
+    N += d.g.n;
+    M += d.g.m;
   }
   if (N + 1 > labels_cap) {
     if (d_labels) cudaFree(d_labels);
@@ -342,16 +466,16 @@ int scc_server::run_batch(std::vector<Request *> &batch) {
   dg.n = (uint32_t)N;
   dg.m = (uint32_t)M;
   if (batch.size() == 1) {
-    Request *r = batch[0];
-    dg.sorted_unique = r->g.sorted_unique;
-    dg.nodes = r->d_off();
-    dg.nodesT = r->d_offT();
-    dg.edges = r->d_adj();
-    dg.edgesT = r->d_adjT();
+    const DevGraph &d = batch[0]->dev();
+    dg.sorted_unique = d.g.sorted_unique;
+    dg.nodes = d.d_off();
+    dg.nodesT = d.d_offT();
+    dg.edges = d.d_adj();
+    dg.edgesT = d.d_adjT();
     rc = scc_ctx_set_segments(ctx, 0, nullptr);
   } else {
     int su = 1;
-    for (Request *r : batch) su &= r->g.sorted_unique ? 1 : 0;
+    for (Request *r : batch) su &= r->g().sorted_unique ? 1 : 0;
     SCK(cudaMemsetAsync(p_off, 0, 8, solve_st), "pack");
     SCK(cudaMemsetAsync(p_offT, 0, 8, solve_st), "pack");
     pack_kernel<<<dim3(64, (unsigned)batch.size()), 256, 0, solve_st>>>(d_desc, p_off, p_adj, p_offT, p_adjT);
@@ -392,7 +516,7 @@ int scc_server::run_batch(std::vector<Request *> &batch) {
   for (size_t i = 0; i < batch.size(); ++i) {
     Request *r = batch[i];
     // labels[0] is overwritten below; slot vbase belongs to the previous graph
-    SCK(cudaMemcpyAsync(r->labels + 1, d_labels + desc[i].vbase + 1, (size_t)r->g.n * 4, cudaMemcpyDeviceToHost,
+    SCK(cudaMemcpyAsync(r->labels + 1, d_labels + desc[i].vbase + 1, (size_t)r->g().n * 4, cudaMemcpyDeviceToHost,
                         solve_st),
         "labels");
   }
@@ -434,13 +558,14 @@ void scc_server::solve_loop() {
       uint64_t nv = 0, ne = 0;
       for (Request *r : ready) {
         if (batch.size() >= max_g) break;
-        if (!batch.empty() && batch[0]->g.n > cfg.solo_vertices) break;  // a large graph goes alone
-        if (!batch.empty() && r->g.n > cfg.solo_vertices) continue;
+        const uint32_t gn = r->g().n, gm = r->g().m;
+        if (!batch.empty() && batch[0]->g().n > cfg.solo_vertices) break;  // a large graph goes alone
+        if (!batch.empty() && gn > cfg.solo_vertices) continue;
         if (!batch.empty() && std::memcmp(r->choice, batch[0]->choice, sizeof(r->choice)) != 0) continue;
-        if (!batch.empty() && (nv + r->g.n > cfg.max_batch_vertices || ne + r->g.m > cfg.max_batch_edges)) continue;
+        if (!batch.empty() && (nv + gn > cfg.max_batch_vertices || ne + gm > cfg.max_batch_edges)) continue;
         batch.push_back(r);
-        nv += r->g.n;
-        ne += r->g.m;
+        nv += gn;
+        ne += gm;
       }
       lk.lock();
       for (Request *r : batch) r->state = RQ_RUNNING;
@@ -538,6 +663,7 @@ int scc_server_set_model(scc_server *s, const float *params, const float *mean, 
   for (auto &kv : s->reqs)
     if (kv.second->state != RQ_DONE)
       return sccb::set_error(SCC_ERR_BUSY, "set the model while no request is in flight");
+  for (auto &kv : s->residents) kv.second->dg.have_choice = false;  // picks belong to the old network
   if (!params) {
     if (s->mlp) scc_mlp_destroy(s->mlp);
     s->mlp = nullptr;
@@ -553,27 +679,134 @@ int scc_server_set_model(scc_server *s, const float *params, const float *mean, 
   return rc;
 }
 
-int scc_server_submit(scc_server *s, const scc_host_csr *g, uint32_t *labels, uint64_t *id) {
-  sccb::clear_error();
-  if (!s || !g || !labels || !id) return sccb::set_error(SCC_ERR_INVALID, "null argument");
+static int check_host_graph(const scc_host_csr *g) {
   if (!g->nodes || !g->nodesT || (g->m && (!g->edges || !g->edgesT)))
     return sccb::set_error(SCC_ERR_INVALID, "graph arrays missing");
   if (g->n >= (1u << 30)) return sccb::set_error(SCC_ERR_CAPACITY, "n must be below 2^30");
   if (g->nodes[g->n + 1] != g->m || g->nodesT[g->n + 1] != g->m)
     return sccb::set_error(SCC_ERR_INVALID, "offsets end at %u/%u, expected m = %u", g->nodes[g->n + 1],
                            g->nodesT[g->n + 1], g->m);
+  return SCC_OK;
+}
+
+int scc_server_register(scc_server *s, const scc_host_csr *g, uint64_t *handle) {
+  sccb::clear_error();
+  if (!s || !g || !handle) return sccb::set_error(SCC_ERR_INVALID, "null argument");
+  int rc = check_host_graph(g);
+  if (rc) return rc;
+  std::unique_ptr<Resident> res(new Resident());
+  res->dg.g = *g;
+  res->dg.bytes = DevGraph::csr_bytes(g->n, g->m);
+  Resident *r = res.get();
+  {
+    std::unique_lock<std::mutex> lk(s->mu);
+    if (s->stopping) return sccb::set_error(SCC_ERR_STATE, "server is stopping");
+    if (r->dg.bytes > s->st.budget_bytes) {
+      ++s->st.rejected;
+      return sccb::set_error(SCC_ERR_REJECTED, "graph needs %llu bytes, the budget is %llu",
+                             (unsigned long long)r->dg.bytes, (unsigned long long)s->st.budget_bytes);
+    }
+    // room comes from evicting idle resident graphs or from requests finishing
+    s->cv_done.wait(lk, [&] { return s->stopping || s->make_room(r->dg.bytes); });
+    if (s->stopping) return sccb::set_error(SCC_ERR_STATE, "server is stopping");
+    s->st.resident_bytes += r->dg.bytes;
+    s->st.peak_resident_bytes = std::max(s->st.peak_resident_bytes, s->st.resident_bytes);
+    r->handle = s->next_handle++;
+    r->uploading = true;
+    r->last_use = ++s->lru_clock;
+    s->residents.emplace(r->handle, std::move(res));
+  }
+  cudaSetDevice(s->cfg.device);
+  cudaError_t e = s->upload(r->dg);
+  if (e == cudaSuccess) e = cudaEventSynchronize(r->dg.uploaded);
+  std::lock_guard<std::mutex> lk(s->mu);
+  r->uploading = false;
+  s->cv_admit.notify_all();
+  if (e != cudaSuccess) {
+    cudaStreamSynchronize(s->copy_st);
+    cudaStreamSynchronize(s->feat_st);
+    s->release_dev(r->dg, s->copy_st);
+    s->st.resident_bytes -= r->dg.bytes;
+    if (r->dg.uploaded) cudaEventDestroy(r->dg.uploaded);
+    if (r->dg.featured) cudaEventDestroy(r->dg.featured);
+    s->residents.erase(r->handle);
+    return srv_fail(e, "register upload");
+  }
+  ++s->st.registered;
+  *handle = r->handle;
+  return SCC_OK;
+}
+
+int scc_server_submit_resident(scc_server *s, uint64_t handle, uint32_t *labels, uint64_t *id) {
+  sccb::clear_error();
+  if (!s || !labels || !id) return sccb::set_error(SCC_ERR_INVALID, "null argument");
+  std::lock_guard<std::mutex> lk(s->mu);
+  if (s->stopping) return sccb::set_error(SCC_ERR_STATE, "server is stopping");
+  auto it = s->residents.find(handle);
+  if (it == s->residents.end())
+    return sccb::set_error(SCC_ERR_INVALID, "unknown graph handle %llu", (unsigned long long)handle);
+  Resident *res = it->second.get();
   std::unique_ptr<Request> r(new Request());
-  r->g = *g;
+  r->res = res;
   r->labels = labels;
-  r->bytes = Request::csr_bytes(g->n, g->m);
+  r->t_submit = Clock::now();
+  ++s->st.submitted;
+  ++res->pending;
+  res->last_use = ++s->lru_clock;
+  r->id = s->next_id++;
+  *id = r->id;
+  Request *rp = r.get();
+  s->reqs.emplace(r->id, std::move(r));
+  if (!res->uploading && res->dg.dmem) {  // on the device: ready at once, no admission needed
+    rp->t_admit = rp->t_submit;
+    rp->state = RQ_READY;
+    s->cv_solve.notify_one();
+  } else {  // evicted: the admission thread uploads it again
+    s->admit_q.push_back(rp);
+    s->cv_admit.notify_one();
+  }
+  return SCC_OK;
+}
+
+int scc_server_unregister(scc_server *s, uint64_t handle) {
+  sccb::clear_error();
+  if (!s) return sccb::set_error(SCC_ERR_INVALID, "null server");
+  std::lock_guard<std::mutex> lk(s->mu);
+  auto it = s->residents.find(handle);
+  if (it == s->residents.end())
+    return sccb::set_error(SCC_ERR_INVALID, "unknown graph handle %llu", (unsigned long long)handle);
+  Resident *r = it->second.get();
+  if (r->pending || r->uploading)
+    return sccb::set_error(SCC_ERR_BUSY, "graph %llu still has %u requests in flight", (unsigned long long)handle,
+                           r->pending);
+  if (r->dg.dmem) {
+    s->evict(r);
+    --s->st.evictions;  // a release, not an eviction
+  }
+  if (r->dg.uploaded) cudaEventDestroy(r->dg.uploaded);
+  if (r->dg.featured) cudaEventDestroy(r->dg.featured);
+  if (r->released) cudaEventDestroy(r->released);
+  s->residents.erase(it);
+  return SCC_OK;
+}
+
+int scc_server_submit(scc_server *s, const scc_host_csr *g, uint32_t *labels, uint64_t *id) {
+  sccb::clear_error();
+  if (!s || !g || !labels || !id) return sccb::set_error(SCC_ERR_INVALID, "null argument");
+  int rc = check_host_graph(g);
+  if (rc) return rc;
+  std::unique_ptr<Request> r(new Request());
+  r->own.g = *g;
+  r->own.bytes = DevGraph::csr_bytes(g->n, g->m);
+  r->labels = labels;
   r->t_submit = Clock::now();
   std::lock_guard<std::mutex> lk(s->mu);
   if (s->stopping) return sccb::set_error(SCC_ERR_STATE, "server is stopping");
   ++s->st.submitted;
-  if (r->bytes > s->st.budget_bytes) {
+  if (r->own.bytes > s->st.budget_bytes) {
     ++s->st.rejected;
     return sccb::set_error(SCC_ERR_REJECTED, "graph needs %llu bytes, the budget is %llu",
-                           (unsigned long long)r->bytes, (unsigned long long)s->st.budget_bytes);
+                           (unsigned long long)r->own.bytes, (unsigned long long)s->st.budget_bytes);
   }
   if (!s->cfg.batching && g->n + 1 > (1u << 30)) return sccb::set_error(SCC_ERR_CAPACITY, "graph too large");
   r->id = s->next_id++;
@@ -646,10 +879,17 @@ int scc_server_stop(scc_server *s) {
   if (s->copy_st) cudaStreamSynchronize(s->copy_st);
   if (s->feat_st) cudaStreamSynchronize(s->feat_st);
   for (auto &kv : s->reqs) {
-    Request *r = kv.second.get();
-    if (r->dmem) cudaFree(r->dmem);
-    if (r->uploaded) cudaEventDestroy(r->uploaded);
-    if (r->featured) cudaEventDestroy(r->featured);
+    DevGraph &d = kv.second->own;
+    if (d.dmem) cudaFree(d.dmem);
+    if (d.uploaded) cudaEventDestroy(d.uploaded);
+    if (d.featured) cudaEventDestroy(d.featured);
+  }
+  for (auto &kv : s->residents) {
+    Resident *r = kv.second.get();
+    if (r->dg.dmem) cudaFree(r->dg.dmem);
+    if (r->dg.uploaded) cudaEventDestroy(r->dg.uploaded);
+    if (r->dg.featured) cudaEventDestroy(r->dg.featured);
+    if (r->released) cudaEventDestroy(r->released);
   }
   for (void *p : {(void *)s->p_off, (void *)s->p_offT, (void *)s->p_adj, (void *)s->p_adjT, (void *)s->d_labels,
                   (void *)s->d_desc, (void *)s->d_nscc})

@@ -1,11 +1,12 @@
 """Serving: the request loop of scc_server_* (include/scc_capi.h) and a
 Poisson-arrival driver that measures per-request latency and throughput.
 
-The server admits graphs by device memory, keeps their CSR resident, and
-batches the requests that are ready whenever the device frees up (continuous
-batching); with a strategy network loaded, each request's options are picked
-by the network and only requests with equal options share a launch.  The
-labels of a request are the same whichever batch it lands in.
+The server admits graphs by device memory, keeps registered graphs' CSR
+resident (evicting idle ones, least recently used first, when an upload needs
+room), and batches the requests that are ready whenever the device frees up
+(continuous batching); with a strategy network loaded, each request's options
+are picked by the network and only requests with equal options share a
+launch.  The labels of a request are the same whichever batch it lands in.
 """
 from __future__ import annotations
 
@@ -42,6 +43,7 @@ class Server:
         check(lib.scc_server_start(C.byref(cfg), C.byref(h)))
         self._h = h
         self._keep = {}  # request id -> (graph, labels) kept alive until retired
+        self._resident = {}  # handle -> registered graph (its host arrays back re-uploads)
         self._lock = threading.Lock()
         if model is not None:
             self.set_model(model)
@@ -62,14 +64,39 @@ class Server:
         check(lib.scc_server_set_model(self._h, params.ctypes.data_as(fp), mean.ctypes.data_as(fp),
                                        scale.ctypes.data_as(fp)))
 
-    def submit(self, g: HostCSR, out: np.ndarray | None = None) -> int:
-        """Queue g; its labels land in `out` (uint32, n+1; e.g. pinned) or a new array."""
-        labels = np.zeros(g.n + 1, np.uint32) if out is None else out
-        if labels.dtype != np.uint32 or labels.size < g.n + 1 or not labels.flags.c_contiguous:
+    def register(self, g: HostCSR) -> int:
+        """Upload g once and keep its CSR resident; returns the handle that
+        submit() accepts in place of a graph."""
+        h = C.c_uint64()
+        check(lib.scc_server_register(self._h, C.byref(g.raw), C.byref(h)))
+        with self._lock:
+            self._resident[h.value] = g
+        return h.value
+
+    def unregister(self, handle: int) -> None:
+        check(lib.scc_server_unregister(self._h, handle))
+        with self._lock:
+            self._resident.pop(handle, None)
+
+    def submit(self, g, out: np.ndarray | None = None) -> int:
+        """Queue g (a HostCSR, uploaded for this request, or a handle from
+        register()); its labels land in `out` (uint32, n+1; e.g. pinned) or a
+        new array."""
+        resident = isinstance(g, (int, np.integer))
+        if resident:
+            with self._lock:
+                graph = self._resident[int(g)]
+        else:
+            graph = g
+        labels = np.zeros(graph.n + 1, np.uint32) if out is None else out
+        if labels.dtype != np.uint32 or labels.size < graph.n + 1 or not labels.flags.c_contiguous:
             raise ValueError("out must be a contiguous uint32 array of n+1 entries")
         rid = C.c_uint64()
-        check(lib.scc_server_submit(self._h, C.byref(g.raw), labels.ctypes.data_as(C.POINTER(C.c_uint32)),
-                                    C.byref(rid)))
+        lp = labels.ctypes.data_as(C.POINTER(C.c_uint32))
+        if resident:
+            check(lib.scc_server_submit_resident(self._h, int(g), lp, C.byref(rid)))
+        else:
+            check(lib.scc_server_submit(self._h, C.byref(g.raw), lp, C.byref(rid)))
         with self._lock:
             self._keep[rid.value] = (g, labels)
         return rid.value

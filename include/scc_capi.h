@@ -209,7 +209,7 @@ typedef struct scc_stats {
   uint32_t n_trim2;        /* vertices removed by trim-2 */
   uint32_t n_fb_elim;      /* vertices eliminated as F∩B or trim-2 (reference countElimmed) */
   uint32_t nscc;           /* number of SCCs */
-  uint32_t largest_scc;    /* size of the largest SCC (0 if not computed) */
+  uint32_t largest_scc;    /* vertices in the largest SCC (tarjan.cpp:155 biggestSCC); 0 only for n = 0 */
   uint32_t pull_sweeps;    /* reach sweeps done in pull (bottom-up) direction */
   uint32_t grid_blocks;    /* persistent grid actually launched */
   uint32_t block_size;
@@ -252,17 +252,21 @@ int scc_batch_solve(scc_ctx *ctx, uint32_t count, const scc_host_csr *graphs, ui
  * buffer (d_labels = NULL) to the host: labels (n+1). */
 int scc_read_labels(scc_ctx *ctx, uint32_t *labels);
 /* No counterpart in the reference (it cudaMallocs everything per call).
- * The whole decomposition for callers that cannot allocate device memory —
- * code running while a stream is captured, plugins whose host framework owns
- * the whole device-memory budget, latency-critical loops that must not hit
- * the allocator's implicit synchronisation.  Needs no context: all scratch
- * lives in one static device array (about 4.7 MB per GPU, held until the
+ * The whole decomposition for callers that cannot allocate device memory:
+ * plugins whose host framework owns the whole device-memory budget and
+ * forbids side allocations, and latency-critical loops that must not hit the
+ * allocator's implicit synchronisation.  Needs no context: all scratch
+ * lives in one static device array (about 5 MB per GPU, held until the
  * process exits), so graphs are limited to 65536 vertices and 4194304 edges
  * (SCC_ERR_CAPACITY beyond).  g: device CSR in the reference layout;
  * d_labels: device (n+1) output or NULL; stream: cudaStream_t or NULL.
+ * Options are validated as for scc_ctx_create.  Returns once the solve has
+ * finished (it waits for `stream` to read the result back).
  * Calls that overlap on the GPU share the array and race; serialise them.
- * The first call on each device does a one-time set-up for that device, so
- * make it before any stream capture. */
+ * The first call on each device does a one-time set-up for that device
+ * (it looks up the array's device address).  cudaDeviceReset invalidates
+ * that set-up: after resetting a device, do not call this entry point on
+ * that device again in the same process. */
 int scc_solve_noalloc(const scc_dev_csr *g, const scc_opts *opts, uint32_t *d_labels, uint32_t *nscc,
                       void *stream);
 /* Enqueue the solve on the context stream without synchronising (capturable
@@ -366,9 +370,10 @@ int scc_mlp_apply(const int32_t *choice, scc_opts *opts);
 /* ---------------------------------------------------------------- server
  * No counterpart in the reference.  A request loop on one device: graphs
  * are admitted while their CSR fits in the memory budget (FIFO), uploaded
- * on a copy stream while earlier work runs, kept resident, and solved in
- * batches of the requests that are ready when the device frees up (one
- * segmented persistent launch per batch; a graph alone is bound in place).
+ * on a copy stream while earlier work runs (or registered once and kept
+ * resident), and solved in batches of the requests that are ready when the
+ * device frees up (one segmented persistent launch per batch; a graph alone
+ * is bound in place).
  * With a strategy network loaded, each request's options come from it and
  * only requests with the same options share a batch. */
 typedef struct scc_server scc_server;
@@ -396,6 +401,9 @@ typedef struct scc_request_info {
 typedef struct scc_server_stats {
   uint64_t submitted, completed, rejected, batches, graphs_batched;
   uint64_t resident_bytes, peak_resident_bytes, budget_bytes;
+  uint64_t registered;  /* graphs registered (scc_server_register) */
+  uint64_t evictions;   /* resident device copies dropped to make room (least recently used first) */
+  uint64_t reuploads;   /* requests of a resident graph that found it evicted and uploaded it again */
 } scc_server_stats;
 void scc_server_cfg_default(scc_server_cfg *cfg);
 int scc_server_start(const scc_server_cfg *cfg, scc_server **out);
@@ -406,6 +414,18 @@ int scc_server_set_model(scc_server *s, const float *params, const float *mean, 
  * the request completes.  SCC_ERR_REJECTED if the graph alone exceeds the
  * memory budget. */
 int scc_server_submit(scc_server *s, const scc_host_csr *g, uint32_t *labels, uint64_t *id);
+/* Resident graphs: upload g once and keep its CSR on the device under
+ * *handle (returns when the upload is done; g's host arrays must stay valid
+ * until scc_server_unregister).  When an upload needs room, resident graphs
+ * with no request in flight are evicted, least recently used first; a later
+ * request of an evicted graph uploads it again from those host arrays.
+ * SCC_ERR_REJECTED if g alone exceeds the budget. */
+int scc_server_register(scc_server *s, const scc_host_csr *g, uint64_t *handle);
+/* Queue a solve of a resident graph (no upload while it stays resident);
+ * labels: host (n+1), valid until the request completes. */
+int scc_server_submit_resident(scc_server *s, uint64_t handle, uint32_t *labels, uint64_t *id);
+/* Drop a resident graph (SCC_ERR_BUSY while requests naming it are in flight). */
+int scc_server_unregister(scc_server *s, uint64_t handle);
 /* SCC_ERR_BUSY while the request runs; otherwise its info, and the request
  * is retired.  A failed solve returns its error code (info->status). */
 int scc_server_poll(scc_server *s, uint64_t id, scc_request_info *info);

@@ -102,3 +102,58 @@ def test_stop_finishes_queued_requests(graphs, alone):
     srv.stop()
     for rid, (ref, _) in zip(ids, alone[:8]):
         assert np.array_equal(keep[rid][1], ref)
+
+
+@pytest.mark.parametrize("batching", [True, False])
+def test_resident_graphs_same_alone_and_mixed_with_uploads(graphs, alone, batching):
+    with Server(0, BASE, batching=batching) as srv:
+        handles = [srv.register(g) for g in graphs[:12]]
+        st0 = srv.stats()
+        # each resident graph twice, interleaved with host graphs uploaded per request
+        items = []
+        for i, h in enumerate(handles):
+            items += [(i, h), (12 + i % (len(graphs) - 12), graphs[12 + i % (len(graphs) - 12)]), (i, h)]
+        ids = [srv.submit(x) for _, x in items]
+        out = [srv.wait(i) for i in ids]
+        st = srv.stats()
+        for h in handles:
+            srv.unregister(h)
+        assert srv.stats()["resident_bytes"] == 0
+    for (gi, _), (labels, info) in zip(items, out):
+        assert np.array_equal(labels, alone[gi][0])
+        assert info["nscc"] == alone[gi][1]
+    assert st0["registered"] == 12 and st["evictions"] == 0 and st["reuploads"] == 0
+    # the resident graphs stayed on the device: only the host graphs were uploaded per request
+    assert st["resident_bytes"] == sum(2 * 4 * (((g.n + 2) + 3) // 4 * 4) + 2 * 4 * ((g.m + 3) // 4 * 4)
+                                       for g in graphs[:12])
+
+
+def test_resident_graphs_evicted_least_recently_used_and_uploaded_again(graphs, alone):
+    big = sorted(range(len(graphs)), key=lambda i: -graphs[i].m)[:3]
+    sizes = [2 * 4 * (((graphs[i].n + 2) + 3) // 4 * 4) + 2 * 4 * ((graphs[i].m + 3) // 4 * 4) for i in big]
+    budget = sizes[0] + sizes[1] + sizes[2] - 1  # two of the three fit, not all three
+    with Server(0, BASE, mem_budget=budget) as srv:
+        h0 = srv.register(graphs[big[0]])
+        h1 = srv.register(graphs[big[1]])
+        srv.wait(srv.submit(h0))                 # h0 used last: h1 is now the least recently used
+        h2 = srv.register(graphs[big[2]])        # needs room: evicts h1
+        st = srv.stats()
+        assert st["evictions"] >= 1 and st["resident_bytes"] <= budget
+        labels, info = srv.wait(srv.submit(h1))  # evicted: uploaded again, labels still exact
+        st2 = srv.stats()
+        l0, _ = srv.wait(srv.submit(h0))
+        l2, _ = srv.wait(srv.submit(h2))
+    assert st2["reuploads"] >= 1
+    assert st2["peak_resident_bytes"] <= budget
+    assert np.array_equal(labels, alone[big[1]][0])
+    assert np.array_equal(l0, alone[big[0]][0]) and np.array_equal(l2, alone[big[2]][0])
+
+
+def test_unknown_or_dropped_handle_is_refused(graphs):
+    with Server(0, BASE) as srv:
+        h = srv.register(graphs[0])
+        srv.unregister(h)
+        with pytest.raises(scc.SCCError):
+            srv.unregister(h)
+        with pytest.raises((scc.SCCError, KeyError)):
+            srv.submit(h)

@@ -1,7 +1,6 @@
 """scc_solve_noalloc: the decomposition for callers that cannot allocate
-device memory (code running under stream capture, plugins whose host owns the
-whole device-memory budget, loops that must avoid the allocator's implicit
-synchronisation).  Its scratch is a static device array shared by all calls,
+device memory (plugins whose host framework owns the whole device-memory
+budget, loops that must avoid the allocator's implicit synchronisation).  Its scratch is a static device array shared by all calls,
 so the test calls it twice in a row — on two different graphs and then on the
 first again — and compares each result, bit-exact, with scc_solve_device's
 (the context-owned-scratch entry point) on the same graph.
@@ -14,7 +13,7 @@ import numpy as np
 import pytest
 
 import gpuscc_code_b200 as scc
-from gpuscc_code_b200._capi import SCC_ERR_CAPACITY, check, lib, scc_dev_csr, scc_opts
+from gpuscc_code_b200._capi import SCC_ERR_CAPACITY, SCC_ERR_INVALID, check, lib, scc_dev_csr, scc_opts
 
 pytestmark = pytest.mark.gpu
 
@@ -77,4 +76,17 @@ def test_noalloc_rejects_graphs_beyond_its_limit():
     rc = lib.scc_solve_noalloc(C.byref(d), C.byref(o), None, C.byref(cnt), None)
     assert rc == SCC_ERR_CAPACITY
     assert b"65536" in lib.scc_last_error()
+    del keep
+
+
+def test_noalloc_rejects_the_options_the_context_rejects():
+    g = scc.gen_rmat(8, 1 << 11, seed=2)
+    d, keep = _device_graph(g)
+    for bad in (dict(occupancy=9), dict(block_size=300), dict(heavy_degree=10), dict(pivot_rule=5)):
+        o = scc.Options(**bad).to_c()
+        cnt = C.c_uint32()
+        rc = lib.scc_solve_noalloc(C.byref(d), C.byref(o), None, C.byref(cnt), None)
+        assert rc == SCC_ERR_INVALID, bad
+        with pytest.raises(scc.SCCError):
+            scc.SCCContext(0, **bad)
     del keep
