@@ -128,3 +128,81 @@ def shard_graphs(weights, world: int) -> list[list[int]]:
 def graph_weight(n: int, m: int) -> int:
     """Bytes the solve of one graph must touch (CSR + transpose + labels)."""
     return 8 * (n + 1) + 8 * m + 4 * n
+
+
+def solve_shard(graphs, rank: int, world: int, solve_fn):
+    """This rank's part of a batch spread over `world` ranks: the graphs of
+    shard_graphs' plan for `rank`, solved by solve_fn(list of graphs) ->
+    [(labels, count)].  Returns {graph index: (labels, count)}; no graph
+    crosses ranks, so the solve itself needs no collective."""
+    plan = shard_graphs([graph_weight(g.n, g.m) for g in graphs], world)
+    mine = plan[rank]
+    res = solve_fn([graphs[i] for i in mine]) if mine else []
+    return dict(zip(mine, res))
+
+
+def gather_results(local: dict, world: int, group=None):
+    """All ranks' {graph index: (labels, count)} merged on every rank (one
+    object all-gather over the process group, after the solves)."""
+    import torch.distributed as dist
+
+    parts = [None] * world
+    dist.all_gather_object(parts, local, group=group)
+    merged = {}
+    for p in parts:
+        merged.update(p)
+    return [merged[i] for i in sorted(merged)]
+
+
+class PeerLeft(RuntimeError):
+    """A rank announced that it left between steps."""
+
+
+class PeerLost(RuntimeError):
+    """A rank neither reached the step nor announced leaving in time."""
+
+
+class RankWatch:
+    """Host-side failure detection between steps of a multi-rank run.
+
+    Each rank records the step it is about to start in the process group's
+    store; before its next launch (and so before any collective of that
+    step) a rank waits, for at most `timeout_s`, until every peer has reached
+    the same step.  A peer that announced leaving raises PeerLeft at once; a
+    peer that went silent raises PeerLost when the wait runs out.  Ranks leave
+    only between steps, with none of their kernels or collectives in flight,
+    so the others learn of it on the host and never launch work that would
+    wait for the missing rank."""
+
+    def __init__(self, store, rank: int, world: int, timeout_s: float = 5.0, poll_s: float = 0.01):
+        self.store, self.rank, self.world = store, rank, world
+        self.timeout_s, self.poll_s = timeout_s, poll_s
+
+    def leave(self) -> None:
+        self.store.set(f"scc_watch/left/{self.rank}", "1")
+
+    def _get(self, key):
+        try:
+            if self.store.check([key]):
+                return self.store.get(key).decode()
+        except Exception:
+            return None
+        return None
+
+    def step(self, i: int) -> None:
+        import time
+
+        self.store.set(f"scc_watch/step/{self.rank}", str(i))
+        deadline = time.monotonic() + self.timeout_s
+        for peer in range(self.world):
+            if peer == self.rank:
+                continue
+            while True:
+                if self._get(f"scc_watch/left/{peer}") is not None:
+                    raise PeerLeft(f"rank {peer} left before step {i}")
+                s = self._get(f"scc_watch/step/{peer}")
+                if s is not None and int(s) >= i:
+                    break
+                if time.monotonic() > deadline:
+                    raise PeerLost(f"rank {peer} did not reach step {i} within {self.timeout_s} s")
+                time.sleep(self.poll_s)

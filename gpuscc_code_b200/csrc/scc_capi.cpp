@@ -119,6 +119,7 @@ int check_opts(const scc_opts *o) {
   if (o->heavy_degree != 0 && o->heavy_degree < 256) return set_error(SCC_ERR_INVALID, "heavy_degree must be >= 256");
   if (o->occupancy != 0 && (o->occupancy < 3 || o->occupancy > 6))
     return set_error(SCC_ERR_INVALID, "occupancy must be 0 or 3..6");
+  if (o->test_stall_us > 10000000u) return set_error(SCC_ERR_INVALID, "test_stall_us must be at most 10 s");
   return SCC_OK;
 }
 
@@ -226,6 +227,9 @@ sccb::Params make_params(scc_ctx *c, uint32_t *out_labels) {
   e.max_iters = o.max_iters ? o.max_iters : (1u << 20);
   e.timeout_ns = (unsigned long long)(o.timeout_ms ? o.timeout_ms : 10000u) * 1000000ull;
   e.trim_first_depth = o.trim_first_depth;
+  e.test_stall_ns = (unsigned long long)o.test_stall_us * 1000ull;
+  // a test cap only shortens the usable part of the (n+1)-entry worklists
+  if (o.test_queue_cap && o.test_queue_cap < s.qcap) s.qcap = o.test_queue_cap;
   // labels are written straight into the caller's device buffer when given
   if (out_labels) s.label = out_labels;
   return p;

@@ -55,6 +55,12 @@ struct Eng {
   __device__ uint32_t rdprv(uint32_t i) { return ldm(prv() + i); }
 
   __device__ bool bar(uint32_t where) {
+    if (P.o.test_stall_ns && k == 1 && blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) {
+      // fault-path test hook: a bounded delay of this CTA's arrival (the
+      // others' barrier waits run out first when timeout_ns is shorter)
+      const unsigned long long t0 = globaltimer_ns();
+      while (globaltimer_ns() - t0 < P.o.test_stall_ns) __nanosleep(1000);
+    }
     if (blockIdx.x == 0) {
       if (threadIdx.x < 16) c->ctr[(k + 1) % 3][threadIdx.x] = 0;
       if (threadIdx.x == 16) c->ctr64[(k + 1) % 3] = 0;

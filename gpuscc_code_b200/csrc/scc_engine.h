@@ -101,6 +101,7 @@ struct EngOpts {
   unsigned long long timeout_ns;
   int32_t trim_first_depth;
   uint32_t pad;
+  unsigned long long test_stall_ns;  // fault-path test hook: last CTA stalls before barrier interval 1 ends
 };
 
 struct Params {

@@ -173,6 +173,8 @@ extern "C" int scc_solve_noalloc(const scc_dev_csr *g, const scc_opts *opts, uin
   e.max_iters = o.max_iters ? o.max_iters : (1u << 20);
   e.timeout_ns = (unsigned long long)(o.timeout_ms ? o.timeout_ms : 10000u) * 1000000ull;
   e.trim_first_depth = o.trim_first_depth;
+  e.test_stall_ns = (unsigned long long)o.test_stall_us * 1000ull;
+  if (o.test_queue_cap && o.test_queue_cap < s.qcap) s.qcap = o.test_queue_cap;
   if (d_labels) s.label = d_labels;  // labels go straight to the caller's buffer
 
   // the array keeps the previous call's contents: reset what must start fresh

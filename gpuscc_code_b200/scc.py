@@ -187,6 +187,8 @@ class Options:
     timeout_ms: int = 0
     trim_first_depth: int = 1
     occupancy: int = 0
+    test_stall_us: int = 0
+    test_queue_cap: int = 0
 
     def to_c(self) -> scc_opts:
         o = scc_opts()

@@ -85,6 +85,16 @@ typedef struct scc_opts {
                               k > 0 = at most k iterations; later partition-aware trims remove the rest */
   int32_t occupancy;       /* register budget of the persistent kernel: 4 = four 256-thread CTAs per SM
                               (64 registers), 3 = three (80 registers); 0 = engine default (4) */
+  /* Fault-path test hooks (0 = off; labels are never affected while off).
+   * test_stall_us: the last CTA of the grid waits this long (a bounded
+   *   %globaltimer spin) before its second grid-barrier arrival, so that the
+   *   other CTAs' bounded barrier waits (timeout_ms) run out: the solve then
+   *   returns SCC_ERR_TIMEOUT and the context stays usable.
+   * test_queue_cap: caps every worklist's usable length (entries) below its
+   *   allocation, so that a push past it reports SCC_ERR_TIMEOUT (queue
+   *   overflow) instead of the reference's silent drop (worklistc.h:79-81). */
+  uint32_t test_stall_us;
+  uint32_t test_queue_cap;
 } scc_opts;
 
 /* Reference defaults: alg TOPO, wcc 0, trim2 0, trim_first 1, block 256, pivot MIN_ID, switch 10;

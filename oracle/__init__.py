@@ -25,7 +25,8 @@ u8p = C.POINTER(C.c_uint8)
 
 
 def build() -> None:
-    """make -C oracle (the C restatement; the reference objects where /root/reference exists)."""
+    """make -C oracle (the C restatement; the reference objects where the reference
+    checkout named by SCC_REFERENCE_DIR exists)."""
     subprocess.run(["make", "-s", "-C", str(HERE)], check=True, capture_output=True)
 
 

@@ -16,6 +16,7 @@ Run in a container that has the reference tree (oracle/_ref built by
 from __future__ import annotations
 
 import json
+import os
 import shutil
 import sys
 from pathlib import Path
@@ -26,7 +27,7 @@ HERE = Path(__file__).resolve().parent
 sys.path.insert(0, str(HERE.parents[1]))
 import oracle  # noqa: E402
 
-REF = Path("/root/reference")
+REF = Path(os.environ.get("SCC_REFERENCE_DIR", "/root/reference"))  # the reference checkout (read only)
 
 
 def write_plain(path: Path, n: int, pairs):
