@@ -261,9 +261,33 @@ int read_ctl(scc_ctx *c) {
   return SCC_OK;
 }
 
+// A segmented graph must hold independent graphs: no edge may leave its
+// source's segment (the first FB round relies on it and runs unranged).
+// Checked on the device whenever a caller's segment table and a graph are
+// both bound; on a violation the segments are dropped.
+int verify_segments(scc_ctx *c) {
+  if (c->nseg <= 1 || !c->have_graph || c->seg_host.back() != c->n + 1) return SCC_OK;
+  CK(c->ctl.ensure(sizeof(sccb::Ctl)), "alloc control block");
+  for (int t = 0; t < 2; ++t) {
+    uint32_t bad = 0;
+    CK(sccb::check_segments(t ? c->d_offT : c->d_off, t ? c->d_adjT : c->d_adj, c->n, c->seg.as<uint32_t>(), c->nseg,
+                            c->ctl.as<uint32_t>(), &bad, c->stream),
+       "segment check");
+    if (bad) {
+      c->nseg = 0;
+      c->seg_host.clear();
+      return set_error(SCC_ERR_INVALID, "an edge of the %s leaves its segment (segments must be independent graphs)",
+                       t ? "transpose" : "graph");
+    }
+  }
+  return SCC_OK;
+}
+
 int launch(scc_ctx *c, uint32_t phase, uint32_t a0 = 0, uint32_t a1 = 0, uint32_t a2 = 0,
            uint32_t *out_labels = nullptr) {
   const sccb::Params p = make_params(c, out_labels);
+  // the grid barrier counts arrivals from zero in every launch
+  CK(cudaMemsetAsync(&p.s.ctl->gs.arrived, 0, sizeof(p.s.ctl->gs.arrived), c->stream), "clear barrier");
   CK(sccb::launch_phase(p, phase, a0, a1, a2, block_size_of(c), c->opts.grid_blocks, c->stream, &c->grid_used,
                         c->opts.occupancy),
      "cooperative launch");
@@ -315,6 +339,12 @@ void fill_stats(scc_ctx *c, scc_stats *st, float ms) {
 }
 
 }  // namespace
+
+// checked and unchecked variants of binding and segment tables (defined below)
+extern "C" {
+static int bind_device_impl(scc_ctx *c, const scc_dev_csr *g, bool verify);
+static int set_segments_impl(scc_ctx *c, uint32_t nseg, const uint32_t *seg_first, bool verify);
+}
 
 extern "C" {
 
@@ -451,7 +481,8 @@ int scc_ctx_upload(scc_ctx *c, const scc_host_csr *g) {
   c->sorted_unique = g->sorted_unique;
   c->have_graph = true;
   c->phase_ready = false;
-  return ensure_state(c);
+  int rs = ensure_state(c);
+  return rs ? rs : verify_segments(c);
 }
 
 int scc_gen_rmat_device(scc_ctx *c, uint32_t scale, uint64_t samples, uint32_t a_ppm, uint32_t b_ppm,
@@ -540,10 +571,10 @@ int scc_gen_batch_device(scc_ctx *c, uint32_t count, uint32_t n_lo, uint32_t n_h
   }
   rc = ensure_state(c);
   if (rc) return rc;
-  return scc_ctx_set_segments(c, count, seg_first);
+  return set_segments_impl(c, count, seg_first, false);  // built here: no edge crosses segments
 }
 
-int scc_ctx_bind_device(scc_ctx *c, const scc_dev_csr *g) {
+static int bind_device_impl(scc_ctx *c, const scc_dev_csr *g, bool verify) {
   sccb::clear_error();
   if (!c || !g) return set_error(SCC_ERR_INVALID, "null argument");
   if (g->n >= (1u << 30)) return set_error(SCC_ERR_CAPACITY, "n must be below 2^30");
@@ -552,7 +583,7 @@ int scc_ctx_bind_device(scc_ctx *c, const scc_dev_csr *g) {
   if (rc) return rc;
   CK(c->ctl.ensure(sizeof(sccb::Ctl)), "alloc control block");
   if (!c->h_ctl) return set_error(SCC_ERR_STATE, "context not initialised");
-  for (int t = 0; t < 2; ++t) {
+  for (int t = 0; verify && t < 2; ++t) {
     uint32_t bad = 0;
     CK(sccb::check_device_csr(t ? g->nodesT : g->nodes, t ? g->edgesT : g->edges, g->n, g->m, c->ctl.as<uint32_t>(),
                               &bad, c->stream),
@@ -570,8 +601,11 @@ int scc_ctx_bind_device(scc_ctx *c, const scc_dev_csr *g) {
   c->sorted_unique = g->sorted_unique;
   c->have_graph = true;
   c->phase_ready = false;
-  return ensure_state(c);
+  rc = ensure_state(c);
+  return (rc || !verify) ? rc : verify_segments(c);
 }
+
+int scc_ctx_bind_device(scc_ctx *c, const scc_dev_csr *g) { return bind_device_impl(c, g, true); }
 
 int scc_ctx_download(scc_ctx *c, scc_host_csr *out) {
   sccb::clear_error();
@@ -628,7 +662,7 @@ int scc_ctx_download_into(scc_ctx *c, uint32_t *nodes, uint32_t *edges, uint32_t
   return SCC_OK;
 }
 
-int scc_ctx_set_segments(scc_ctx *c, uint32_t nseg, const uint32_t *seg_first) {
+static int set_segments_impl(scc_ctx *c, uint32_t nseg, const uint32_t *seg_first, bool verify) {
   sccb::clear_error();
   if (!c) return set_error(SCC_ERR_INVALID, "null context");
   if (nseg == 0) {
@@ -644,10 +678,15 @@ int scc_ctx_set_segments(scc_ctx *c, uint32_t nseg, const uint32_t *seg_first) {
   if (rc) return rc;
   c->seg_host.assign(seg_first, seg_first + nseg + 1);
   CK(c->seg.ensure(((size_t)nseg + 1) * 4), "alloc segments");
-  CK(cudaMemcpy(c->seg.p, seg_first, ((size_t)nseg + 1) * 4, cudaMemcpyHostToDevice), "upload segments");
+  CK(cudaMemcpyAsync(c->seg.p, c->seg_host.data(), ((size_t)nseg + 1) * 4, cudaMemcpyHostToDevice, c->stream),
+     "upload segments");
   c->nseg = nseg;
   c->phase_ready = false;
-  return SCC_OK;
+  return verify ? verify_segments(c) : SCC_OK;
+}
+
+int scc_ctx_set_segments(scc_ctx *c, uint32_t nseg, const uint32_t *seg_first) {
+  return set_segments_impl(c, nseg, seg_first, true);
 }
 
 int scc_solve_enqueue(scc_ctx *c, uint32_t *d_labels) {
@@ -776,8 +815,9 @@ int scc_batch_solve(scc_ctx *c, uint32_t count, const scc_host_csr *graphs, uint
   int rc = scc_batch_pack(count, graphs, &packed, seg.data());
   if (rc) return rc;
   std::vector<uint32_t> all((size_t)packed.n + 1);
+  scc_ctx_set_segments(c, 0, nullptr);  // no stale table is checked against the packed graph
   rc = scc_ctx_upload(c, &packed);
-  if (!rc) rc = scc_ctx_set_segments(c, count, seg.data());
+  if (!rc) rc = set_segments_impl(c, count, seg.data(), false);  // packed here: no edge crosses segments
   uint32_t total = 0;
   if (!rc) rc = scc_solve(c, all.data(), &total, nullptr);
   scc_ctx_set_segments(c, 0, nullptr);
@@ -965,3 +1005,12 @@ int scc_get_labels(scc_ctx *c, uint32_t *labels, uint32_t *nscc) {
 }
 
 }  // extern "C"
+
+namespace sccb {
+// For graphs packed by this library (valid by construction, or checked when
+// they were uploaded): no device checks, no host synchronisation.
+int ctx_bind_unchecked(scc_ctx *c, const scc_dev_csr *g) { return bind_device_impl(c, g, false); }
+int ctx_set_segments_unchecked(scc_ctx *c, uint32_t nseg, const uint32_t *seg_first) {
+  return set_segments_impl(c, nseg, seg_first, false);
+}
+}  // namespace sccb

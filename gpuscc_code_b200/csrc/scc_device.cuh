@@ -62,18 +62,28 @@ __device__ __forceinline__ void bit_clear(uint32_t *bm, uint32_t v) {
 }
 
 // ------------------------------------------------------ grid barrier
-// Sense-less generation barrier for a cooperative (co-resident) grid.  The
-// wait is bounded by `timeout_ns` of %globaltimer; on expiry the CTA records
-// kErrBarrierTimeout and leaves the barrier, and every later barrier returns
-// false at once so the whole grid drains and the kernel exits.
+// Counting barrier for a cooperative (co-resident) grid.  `arrived` only
+// grows during a launch (the host clears it before every launch): barrier
+// number k of the launch is passed once it reaches (k+1) * gridDim.x, so
+// the last CTA to arrive has nothing to reset and the others leave as soon
+// as its arrival is visible.  The wait is bounded by `timeout_ns` of
+// %globaltimer; on expiry the CTA records kErrBarrierTimeout and leaves the
+// barrier, and every later barrier returns false at once so the whole grid
+// drains and the kernel exits.
 struct GridSync {
-  uint32_t count;
-  uint32_t gen;
+  unsigned long long arrived;
   uint32_t err;
   uint32_t err_where;
 };
 
-__device__ __forceinline__ bool grid_barrier(GridSync *gs, uint64_t timeout_ns, uint32_t where) {
+__device__ __forceinline__ unsigned long long ld_acquire64(const unsigned long long *p) {
+  unsigned long long v;
+  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ bool grid_barrier(GridSync *gs, unsigned long long target, uint64_t timeout_ns,
+                                             uint32_t where) {
   __shared__ uint32_t s_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -81,18 +91,13 @@ __device__ __forceinline__ bool grid_barrier(GridSync *gs, uint64_t timeout_ns, 
     if (ld_acquire(&gs->err) != 0) {
       ok = 0;
     } else {
-      const uint32_t gen = ld_acquire(&gs->gen);
-      __threadfence();
-      const uint32_t arrived = atomicAdd(&gs->count, 1u);
-      if (arrived == gridDim.x - 1) {
-        atomicExch(&gs->count, 0u);
-        __threadfence();
-        atomicAdd(&gs->gen, 1u);
-      } else {
+      __threadfence();  // this CTA's writes (ordered before thread 0 by the CTA barrier) go first
+      atomicAdd(&gs->arrived, 1ull);
+      if (ld_acquire64(&gs->arrived) < target) {
         const uint64_t t0 = globaltimer_ns();
         uint32_t spins = 0;
-        while (ld_acquire(&gs->gen) == gen) {
-          __nanosleep(64);
+        while (ld_acquire64(&gs->arrived) < target) {
+          __nanosleep(32);
           if ((++spins & 63u) == 0) {
             if (ld_acquire(&gs->err) != 0) { ok = 0; break; }
             if (globaltimer_ns() - t0 > timeout_ns) {

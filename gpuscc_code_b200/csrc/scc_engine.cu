@@ -65,7 +65,8 @@ struct Eng {
       if (threadIdx.x < 16) c->ctr[(k + 1) % 3][threadIdx.x] = 0;
       if (threadIdx.x == 16) c->ctr64[(k + 1) % 3] = 0;
     }
-    const bool ok = grid_barrier(reinterpret_cast<GridSync *>(&c->gs), P.o.timeout_ns, where);
+    const bool ok = grid_barrier(reinterpret_cast<GridSync *>(&c->gs), (unsigned long long)(k + 1) * gridDim.x,
+                                 P.o.timeout_ns, where);
     ++k;
     return ok;
   }
@@ -1848,6 +1849,39 @@ __global__ void scc_check_edges_kernel(const uint32_t *adj, uint32_t n, uint32_t
     const uint32_t u = adj[i];
     if (u < 1 || u > n) atomicOr(bad, 2u);
   }
+}
+
+// Segment sanity for packed graphs: every edge stays inside its source's
+// segment (seg: nseg+1 first ids, seg[nseg] = n+1).  A thread per vertex.
+__global__ void scc_check_segments_kernel(const uint32_t *off, const uint32_t *adj, uint32_t n, const uint32_t *seg,
+                                          uint32_t nseg, uint32_t *bad) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x + 1; v <= n; v += gridDim.x * blockDim.x) {
+    uint32_t lo = 0, hi = nseg - 1;  // largest s with seg[s] <= v
+    while (lo < hi) {
+      const uint32_t mid = (lo + hi + 1) >> 1;
+      if (seg[mid] <= v) lo = mid;
+      else hi = mid - 1;
+    }
+    const uint32_t first = seg[lo], past = seg[lo + 1];
+    for (uint32_t e = off[v]; e < off[v + 1]; ++e) {
+      const uint32_t u = adj[e];
+      if (u < first || u >= past) {
+        atomicOr(bad, 4u);
+        break;
+      }
+    }
+  }
+}
+
+cudaError_t check_segments(const uint32_t *off, const uint32_t *adj, uint32_t n, const uint32_t *seg, uint32_t nseg,
+                           uint32_t *d_bad, uint32_t *h_bad, cudaStream_t st) {
+  cudaError_t e = cudaMemsetAsync(d_bad, 0, 4, st);
+  if (e != cudaSuccess) return e;
+  if (n && nseg) scc_check_segments_kernel<<<148 * 8, 256, 0, st>>>(off, adj, n, seg, nseg, d_bad);
+  e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpyAsync(h_bad, d_bad, 4, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  return e;
 }
 
 cudaError_t check_device_csr(const uint32_t *off, const uint32_t *adj, uint32_t n, uint32_t m, uint32_t *d_bad,

@@ -8,7 +8,8 @@
 namespace sccb {
 
 struct GridSyncH {
-  uint32_t count, gen, err, err_where;
+  unsigned long long arrived;  // barrier arrivals of the current launch (cleared before each launch)
+  uint32_t err, err_where;
 };
 
 // Device control block.  One per context, cleared by scc_phase_begin / the
@@ -150,6 +151,10 @@ cudaError_t launch_ranges(const Params &p, uint32_t *d_ranges, cudaStream_t stre
 // is nonzero on a violation.  d_bad: 4 bytes of device scratch.
 cudaError_t check_device_csr(const uint32_t *off, const uint32_t *adj, uint32_t n, uint32_t m, uint32_t *d_bad,
                              uint32_t *h_bad, cudaStream_t st);
+// Checks that no edge leaves its source's segment (seg: device, nseg+1
+// first ids); *h_bad is nonzero on a violation.
+cudaError_t check_segments(const uint32_t *off, const uint32_t *adj, uint32_t n, const uint32_t *seg, uint32_t nseg,
+                           uint32_t *d_bad, uint32_t *h_bad, cudaStream_t st);
 
 }  // namespace sccb
 namespace sccg {

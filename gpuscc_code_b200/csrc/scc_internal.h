@@ -12,6 +12,10 @@ int set_error(int code, const char *fmt, ...);
 void clear_error();
 // Validates engine options (every solve entry point accepts the same set).
 int check_opts(const scc_opts *o);
+// Binding and segment table without the device checks, for graphs this
+// library packed or validated itself (the request server).
+int ctx_bind_unchecked(scc_ctx *c, const scc_dev_csr *g);
+int ctx_set_segments_unchecked(scc_ctx *c, uint32_t nseg, const uint32_t *seg_first);
 
 // 1-based pairs -> reference-layout CSR + transpose (sorted, deduplicated).
 int build_csr(uint32_t n, uint64_t ne, const uint32_t *src, const uint32_t *dst, bool drop_self, scc_host_csr *out);

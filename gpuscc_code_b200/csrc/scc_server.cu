@@ -105,6 +105,11 @@ struct DevGraph {
   const uint32_t *d_adj() const { return d_offT() + pad4(g.n + 2); }
   const uint32_t *d_adjT() const { return d_adj() + pad4(g.m); }
   static uint64_t csr_bytes(uint32_t n, uint32_t m) { return (2 * pad4(n + 2) + 2 * pad4(m)) * 4; }
+  // the allocation also holds the 16-byte flag of the upload's CSR check
+  static uint64_t alloc_bytes(uint32_t n, uint32_t m) { return csr_bytes(n, m) + 16; }
+  uint32_t *check_flag() const {
+    return reinterpret_cast<uint32_t *>(static_cast<char *>(dmem) + csr_bytes(g.n, g.m));
+  }
 };
 
 // A registered graph: the caller's host arrays (valid until unregistered)
@@ -167,7 +172,7 @@ struct scc_server {
   void solve_loop();
   int run_batch(std::vector<Request *> &batch);
   int choose(std::vector<Request *> &ready);
-  cudaError_t upload(DevGraph &d);
+  cudaError_t upload(DevGraph &d, bool *invalid);
   cudaError_t start_features(DevGraph &d);
   bool make_room(uint64_t bytes);
   void evict(Resident *r);
@@ -197,7 +202,7 @@ int srv_fail(cudaError_t e, const char *what) {
 // Pool allocation + upload of d's host arrays on the copy stream; with a
 // network loaded, the graph's feature pass follows on its own stream.
 // Called without the lock; d.dmem is published by the caller.
-cudaError_t scc_server::upload(DevGraph &d) {
+cudaError_t scc_server::upload(DevGraph &d, bool *invalid) {
   void *mem = nullptr;
   cudaError_t e = cudaMallocFromPoolAsync(&mem, d.bytes, pool, copy_st);
   if (e != cudaSuccess) return e;
@@ -212,6 +217,16 @@ cudaError_t scc_server::upload(DevGraph &d) {
     e = cudaMemcpyAsync(const_cast<uint32_t *>(d.d_adjT()), d.g.edgesT, mb, cudaMemcpyHostToDevice, copy_st);
   if (e == cudaSuccess && !d.uploaded) e = cudaEventCreateWithFlags(&d.uploaded, cudaEventDisableTiming);
   if (e == cudaSuccess) e = cudaEventRecord(d.uploaded, copy_st);
+  // the kernels trust the layout: each uploaded copy is checked once here,
+  // so the solver binds it (and batches packed from it) without checks
+  *invalid = false;
+  for (int t = 0; e == cudaSuccess && t < 2; ++t) {
+    uint32_t bad = 0;
+    e = sccb::check_device_csr(t ? d.d_offT() : d.d_off(), t ? d.d_adjT() : d.d_adj(), d.g.n, d.g.m, d.check_flag(),
+                               &bad, copy_st);
+    if (e == cudaSuccess && bad) *invalid = true;
+  }
+  if (*invalid) return e;
   // the features are computed behind the upload with nothing waiting for them
   // (the next uploads go on): the solver reads the accumulators when it forms
   // the batch that takes the graph
@@ -316,20 +331,22 @@ void scc_server::admit_loop() {
     st.peak_resident_bytes = std::max(st.peak_resident_bytes, st.resident_bytes);
     r->state = RQ_UPLOADING;
     lk.unlock();
-    const cudaError_t e = upload(d);
+    bool invalid = false;
+    const cudaError_t e = upload(d, &invalid);
     lk.lock();
     if (r->res) {
       r->res->uploading = false;
       cv_admit.notify_all();
     }
-    if (e != cudaSuccess) {
-      sccb::set_error(SCC_ERR_CUDA, "upload: %s", cudaGetErrorString(e));
+    if (e != cudaSuccess || invalid) {
+      if (invalid) sccb::set_error(SCC_ERR_INVALID, "uploaded graph is malformed");
+      else sccb::set_error(SCC_ERR_CUDA, "upload: %s", cudaGetErrorString(e));
       cudaStreamSynchronize(copy_st);  // nothing may still write into the allocation when it is freed
       cudaStreamSynchronize(feat_st);
       release_dev(d, copy_st);
       if (r->res) st.resident_bytes -= d.bytes;  // a host graph's bytes are returned by finish
       lk.unlock();
-      finish(r, e == cudaErrorMemoryAllocation ? SCC_ERR_NOMEM : SCC_ERR_CUDA);
+      finish(r, invalid ? SCC_ERR_INVALID : e == cudaErrorMemoryAllocation ? SCC_ERR_NOMEM : SCC_ERR_CUDA);
       lk.lock();
       continue;
     }
@@ -472,7 +489,7 @@ int scc_server::run_batch(std::vector<Request *> &batch) {
     dg.nodesT = d.d_offT();
     dg.edges = d.d_adj();
     dg.edgesT = d.d_adjT();
-    rc = scc_ctx_set_segments(ctx, 0, nullptr);
+    rc = sccb::ctx_set_segments_unchecked(ctx, 0, nullptr);
   } else {
     int su = 1;
     for (Request *r : batch) su &= r->g().sorted_unique ? 1 : 0;
@@ -489,14 +506,15 @@ int scc_server::run_batch(std::vector<Request *> &batch) {
     for (size_t i = 0; i < batch.size(); ++i) seg[i] = desc[i].vbase + 1;
     seg[batch.size()] = (uint32_t)N + 1;
     rc = 0;
-    // segments are set after binding (binding checks the CSR on the solve stream)
-    int brc = scc_ctx_bind_device(ctx, &dg);
+    // every member was checked at its upload and the pack kernel keeps each
+    // graph on its own ids: bind and segment without device checks
+    int brc = sccb::ctx_bind_unchecked(ctx, &dg);
     if (brc) return brc;
-    rc = scc_ctx_set_segments(ctx, (uint32_t)batch.size(), seg.data());
+    rc = sccb::ctx_set_segments_unchecked(ctx, (uint32_t)batch.size(), seg.data());
     if (rc) return rc;
   }
   if (batch.size() == 1) {
-    rc = scc_ctx_bind_device(ctx, &dg);
+    rc = sccb::ctx_bind_unchecked(ctx, &dg);
     if (rc) return rc;
   }
   uint32_t nscc = 0;
@@ -696,7 +714,7 @@ int scc_server_register(scc_server *s, const scc_host_csr *g, uint64_t *handle) 
   if (rc) return rc;
   std::unique_ptr<Resident> res(new Resident());
   res->dg.g = *g;
-  res->dg.bytes = DevGraph::csr_bytes(g->n, g->m);
+  res->dg.bytes = DevGraph::alloc_bytes(g->n, g->m);
   Resident *r = res.get();
   {
     std::unique_lock<std::mutex> lk(s->mu);
@@ -717,12 +735,13 @@ int scc_server_register(scc_server *s, const scc_host_csr *g, uint64_t *handle) 
     s->residents.emplace(r->handle, std::move(res));
   }
   cudaSetDevice(s->cfg.device);
-  cudaError_t e = s->upload(r->dg);
-  if (e == cudaSuccess) e = cudaEventSynchronize(r->dg.uploaded);
+  bool invalid = false;
+  cudaError_t e = s->upload(r->dg, &invalid);
+  if (e == cudaSuccess && !invalid) e = cudaEventSynchronize(r->dg.uploaded);
   std::lock_guard<std::mutex> lk(s->mu);
   r->uploading = false;
   s->cv_admit.notify_all();
-  if (e != cudaSuccess) {
+  if (e != cudaSuccess || invalid) {
     cudaStreamSynchronize(s->copy_st);
     cudaStreamSynchronize(s->feat_st);
     s->release_dev(r->dg, s->copy_st);
@@ -730,6 +749,7 @@ int scc_server_register(scc_server *s, const scc_host_csr *g, uint64_t *handle) 
     if (r->dg.uploaded) cudaEventDestroy(r->dg.uploaded);
     if (r->dg.featured) cudaEventDestroy(r->dg.featured);
     s->residents.erase(r->handle);
+    if (invalid) return sccb::set_error(SCC_ERR_INVALID, "graph is malformed (offsets or neighbour ids)");
     return srv_fail(e, "register upload");
   }
   ++s->st.registered;
@@ -797,7 +817,7 @@ int scc_server_submit(scc_server *s, const scc_host_csr *g, uint32_t *labels, ui
   if (rc) return rc;
   std::unique_ptr<Request> r(new Request());
   r->own.g = *g;
-  r->own.bytes = DevGraph::csr_bytes(g->n, g->m);
+  r->own.bytes = DevGraph::alloc_bytes(g->n, g->m);
   r->labels = labels;
   r->t_submit = Clock::now();
   std::lock_guard<std::mutex> lk(s->mu);

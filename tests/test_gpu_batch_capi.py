@@ -10,6 +10,7 @@ import gpuscc_code_b200 as scc
 from gpuscc_code_b200 import _capi
 from gpuscc_code_b200.batch import pack
 from gpu_util import oracle_labels
+import oracle
 
 
 def graphs():
@@ -54,3 +55,24 @@ def test_batch_solve_equals_each_graph_alone():
             for g, o, c in zip(gs, outs, counts):
                 ref, rcnt = oracle_labels(g)
                 assert np.array_equal(o, ref) and c == rcnt
+
+
+@pytest.mark.gpu
+def test_segment_table_with_a_crossing_edge_is_refused():
+    # two 3-vertex graphs packed side by side, plus one edge 2 -> 5 across them
+    src = np.array([1, 2, 3, 4, 5, 6, 2], np.uint32)
+    dst = np.array([2, 3, 1, 5, 6, 4, 5], np.uint32)
+    g = scc.csr_from_edges(6, src, dst)
+    with scc.SCCContext(0) as ctx:
+        ctx.upload(g)
+        with pytest.raises(scc.SCCError) as ei:
+            ctx.set_segments(np.array([1, 4, 7], np.uint32))
+        assert ei.value.code == -1 and "segment" in str(ei.value)
+        labels, cnt, _ = ctx.solve()  # the table was dropped: one graph again
+        ref, rcnt = oracle.tarjan_labels(g.n, g.nodes, g.edges)
+        assert cnt == rcnt and np.array_equal(labels, ref)
+        ok = scc.csr_from_edges(6, src[:6], dst[:6])
+        ctx.upload(ok)
+        ctx.set_segments(np.array([1, 4, 7], np.uint32))
+        labels, cnt, _ = ctx.solve()
+        assert cnt == 2 and list(labels) == [0, 1, 1, 1, 4, 4, 4]

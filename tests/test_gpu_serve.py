@@ -104,6 +104,23 @@ def test_stop_finishes_queued_requests(graphs, alone):
         assert np.array_equal(keep[rid][1], ref)
 
 
+def _dev_bytes(g):
+    """Device bytes of one uploaded graph: offsets and lists of both directions
+    (4-entry padded) and the 16-byte flag of its upload check."""
+    pad4 = lambda x: (x + 3) // 4 * 4
+    return 2 * 4 * pad4(g.n + 2) + 2 * 4 * pad4(g.m) + 16
+
+
+def test_malformed_graph_is_refused_at_registration():
+    nodes = np.array([0, 0, 1, 2], np.uint32)
+    bad = scc.HostCSR.from_arrays(nodes, np.array([2, 7], np.uint32), nodes, np.array([2, 1], np.uint32))
+    with Server(0, BASE) as srv:
+        with pytest.raises(scc.SCCError) as ei:
+            srv.register(bad)
+        assert ei.value.code == -1
+        assert srv.stats()["resident_bytes"] == 0
+
+
 @pytest.mark.parametrize("batching", [True, False])
 def test_resident_graphs_same_alone_and_mixed_with_uploads(graphs, alone, batching):
     with Server(0, BASE, batching=batching) as srv:
@@ -124,13 +141,12 @@ def test_resident_graphs_same_alone_and_mixed_with_uploads(graphs, alone, batchi
         assert info["nscc"] == alone[gi][1]
     assert st0["registered"] == 12 and st["evictions"] == 0 and st["reuploads"] == 0
     # the resident graphs stayed on the device: only the host graphs were uploaded per request
-    assert st["resident_bytes"] == sum(2 * 4 * (((g.n + 2) + 3) // 4 * 4) + 2 * 4 * ((g.m + 3) // 4 * 4)
-                                       for g in graphs[:12])
+    assert st["resident_bytes"] == sum(_dev_bytes(g) for g in graphs[:12])
 
 
 def test_resident_graphs_evicted_least_recently_used_and_uploaded_again(graphs, alone):
     big = sorted(range(len(graphs)), key=lambda i: -graphs[i].m)[:3]
-    sizes = [2 * 4 * (((graphs[i].n + 2) + 3) // 4 * 4) + 2 * 4 * ((graphs[i].m + 3) // 4 * 4) for i in big]
+    sizes = [_dev_bytes(graphs[i]) for i in big]
     budget = sizes[0] + sizes[1] + sizes[2] - 1  # two of the three fit, not all three
     with Server(0, BASE, mem_budget=budget) as srv:
         h0 = srv.register(graphs[big[0]])
