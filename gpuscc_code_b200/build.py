@@ -10,6 +10,7 @@ from __future__ import annotations
 import os
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 from pathlib import Path
 
 PKG = Path(__file__).resolve().parent
@@ -47,7 +48,7 @@ def build(force: bool = False, verbose_ptxas: bool = False) -> Path:
     BUILD.mkdir(exist_ok=True)
     BIN.mkdir(exist_ok=True)
     hdrs = [CSRC / h for h in HEADERS] + [INCLUDE / "scc_capi.h"]
-    objs = []
+    objs, jobs = [], []
     for src in CU_SOURCES:
         s = CSRC / src
         o = BUILD / (s.stem + ".o")
@@ -56,15 +57,18 @@ def build(force: bool = False, verbose_ptxas: bool = False) -> Path:
                    "-I", str(CSRC), "-c", str(s), "-o", str(o)]
             if verbose_ptxas:
                 cmd.insert(-4, "-Xptxas=-v")
-            _run(cmd)
+            jobs.append(cmd)
         objs.append(o)
     for src in CPP_SOURCES:
         s = CSRC / src
         o = BUILD / (s.stem + ".o")
         if force or _stale(o, [s] + hdrs):
-            _run(["g++", "-O2", "-std=c++17", "-fPIC", "-pthread", "-I", str(INCLUDE), "-I", str(CSRC),
-                  "-I", str(CUDA_HOME / "include"), "-c", str(s), "-o", str(o)])
+            jobs.append(["g++", "-O2", "-std=c++17", "-fPIC", "-pthread", "-I", str(INCLUDE), "-I", str(CSRC),
+                         "-I", str(CUDA_HOME / "include"), "-c", str(s), "-o", str(o)])
         objs.append(o)
+    # independent translation units compile side by side
+    with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as ex:
+        list(ex.map(_run, jobs))
     if force or _stale(LIB, objs):
         _run([NVCC, *ARCH, "-shared", "-o", str(LIB), *map(str, objs), "-Xcompiler", "-pthread"])
     main = CSRC / "apps" / "scc_main.cpp"

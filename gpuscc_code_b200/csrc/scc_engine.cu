@@ -48,13 +48,13 @@ struct Eng {
   __device__ explicit Eng(const Params &p) : P(p), c(p.s.ctl), k(0), list_mode(0), act_count(0), act_sel(0) {}
 
   // ------------------------------------------------------------ plumbing
-  __device__ uint32_t *cur() { return c->ctr[k % 3]; }
-  __device__ uint32_t *prv() { return c->ctr[(k + 2) % 3]; }
-  __device__ unsigned long long *cur64() { return &c->ctr64[k % 3]; }
-  __device__ unsigned long long *prv64() { return &c->ctr64[(k + 2) % 3]; }
-  __device__ uint32_t rdprv(uint32_t i) { return ldm(prv() + i); }
+  __device__ __forceinline__ uint32_t *cur() { return c->ctr[k % 3]; }
+  __device__ __forceinline__ uint32_t *prv() { return c->ctr[(k + 2) % 3]; }
+  __device__ __forceinline__ unsigned long long *cur64() { return &c->ctr64[k % 3]; }
+  __device__ __forceinline__ unsigned long long *prv64() { return &c->ctr64[(k + 2) % 3]; }
+  __device__ __forceinline__ uint32_t rdprv(uint32_t i) { return ldm(prv() + i); }
 
-  __device__ bool bar(uint32_t where) {
+  __device__ __forceinline__ bool bar(uint32_t where) {
     if (P.o.test_stall_ns && k == 1 && blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) {
       // fault-path test hook: a bounded delay of this CTA's arrival (the
       // others' barrier waits run out first when timeout_ns is shorter)
@@ -70,16 +70,16 @@ struct Eng {
     ++k;
     return ok;
   }
-  __device__ void refresh_mode() {
+  __device__ __forceinline__ void refresh_mode() {
     list_mode = ldm(&c->list_mode);
     act_count = ldm(&c->act_count);
     act_sel = ldm(&c->act_sel);
   }
-  __device__ uint32_t *err() { return &c->gs.err; }
-  __device__ void fail(uint32_t bits) { atomicOr(&c->gs.err, bits); }
-  __device__ bool is_lead() { return blockIdx.x == 0 && threadIdx.x == 0; }
+  __device__ __forceinline__ uint32_t *err() { return &c->gs.err; }
+  __device__ __forceinline__ void fail(uint32_t bits) { atomicOr(&c->gs.err, bits); }
+  __device__ __forceinline__ bool is_lead() { return blockIdx.x == 0 && threadIdx.x == 0; }
   // CTA 0 / thread 0 accumulates the time since t0 under profile slot `slot`
-  __device__ void prof(uint32_t slot, unsigned long long t0, uint32_t a = 0, uint32_t b = 0) {
+  __device__ __forceinline__ void prof(uint32_t slot, unsigned long long t0, uint32_t a = 0, uint32_t b = 0) {
     if (is_lead()) {
       const unsigned long long dt = globaltimer_ns() - t0;
       c->prof_ns[slot] += dt;
@@ -99,7 +99,7 @@ struct Eng {
   // Lanes whose ids share a bitmap word combine into one atomicOr instead of
   // 32 serialised ones.  aligned: lane i holds id 32*w + i of a single word w
   // (full-mode for_vertices), so one ballot forms the word.
-  __device__ void warp_set_bits(uint32_t *bm, uint32_t v, bool pred, bool aligned) {
+  __device__ __forceinline__ void warp_set_bits(uint32_t *bm, uint32_t v, bool pred, bool aligned) {
     if (aligned) {
       const uint32_t bits = __ballot_sync(kFull, pred);
       if (bits && lane_id() == 0) atomicOr(bm + (v >> 5), bits);
@@ -114,7 +114,7 @@ struct Eng {
   }
 
   // block-reduced atomicAdd into a global counter
-  __device__ void add_count(uint32_t *dst, uint32_t x) {
+  __device__ __forceinline__ void add_count(uint32_t *dst, uint32_t x) {
     const uint32_t s = block_sum(x);
     if (threadIdx.x == 0 && s) atomicAdd(dst, s);
   }
@@ -124,22 +124,22 @@ struct Eng {
   // components, so a giant SCC costs one global atomic per CTA, not one per
   // warp.  Running totals only grow, so the largest total any add returns
   // is the largest component.
-  __device__ void size_flush(uint32_t p, uint32_t cnt) {
-    const uint32_t tot = atomicAdd(P.s.sccsize + p, cnt) + cnt;
+  __device__ __forceinline__ void size_flush(const EngState &s, uint32_t p, uint32_t cnt) {
+    const uint32_t tot = atomicAdd(s.sccsize + p, cnt) + cnt;
     if (tot > ldm(&c->largest_fb)) atomicMax(&c->largest_fb, tot);
   }
-  __device__ void size_add(uint32_t *s_szkey, uint32_t *s_szcnt, uint32_t p, uint32_t cnt) {
+  __device__ __forceinline__ void size_add(const EngState &s, uint32_t *s_szkey, uint32_t *s_szcnt, uint32_t p, uint32_t cnt) {
     const uint32_t h = p % kSizeCache;
     uint32_t owner = s_szkey[h];
     if (owner == kNone) owner = atomicCAS(&s_szkey[h], kNone, p) == kNone ? p : s_szkey[h];
     if (owner == p) atomicAdd(&s_szcnt[h], cnt);
-    else size_flush(p, cnt);
+    else size_flush(s, p, cnt);
   }
 
-  __device__ uint32_t gtid() const { return blockIdx.x * BS + threadIdx.x; }
-  __device__ uint32_t gstride() const { return gridDim.x * BS; }
-  __device__ uint32_t gwarp() const { return (blockIdx.x * BS + threadIdx.x) >> 5; }
-  __device__ uint32_t nwarps() const { return (gridDim.x * BS) >> 5; }
+  __device__ __forceinline__ uint32_t gtid() const { return blockIdx.x * BS + threadIdx.x; }
+  __device__ __forceinline__ uint32_t gstride() const { return gridDim.x * BS; }
+  __device__ __forceinline__ uint32_t gwarp() const { return (blockIdx.x * BS + threadIdx.x) >> 5; }
+  __device__ __forceinline__ uint32_t nwarps() const { return (gridDim.x * BS) >> 5; }
 
   // Calls f(v, valid) for every vertex of the current sweep set, all 32
   // lanes of a warp together (valid = false pads the last block), then
@@ -147,7 +147,7 @@ struct Eng {
   // iterations, so after() may __syncthreads).  Full mode covers ids
   // 0 .. nwords*32-1 so that a warp owns exactly one bitmap word.
   template <class F, class H>
-  __device__ void for_vertices(F &&f, H &&after) {
+  __device__ __forceinline__ void for_vertices(F &&f, H &&after) {
     if (list_mode) {
       const uint32_t *lst = P.s.act[act_sel];
       const uint32_t cnt = act_count;
@@ -169,7 +169,7 @@ struct Eng {
     }
   }
   template <class F>
-  __device__ void for_vertices(F &&f) {
+  __device__ __forceinline__ void for_vertices(F &&f) {
     for_vertices(f, [] {});
   }
 
@@ -182,7 +182,7 @@ struct Eng {
   // iterations ahead and the per-vertex loads of the next entry are in
   // flight while f runs on the current one.  Whole CTAs iterate together.
   template <class L, class F>
-  __device__ void for_list_pf(const uint32_t *lst, uint32_t cnt, L &&load, F &&f) {
+  __device__ __forceinline__ void for_list_pf(const uint32_t *lst, uint32_t cnt, L &&load, F &&f) {
     const uint32_t lim = (cnt + BS - 1u) / BS * BS;
     const uint32_t stride = gstride();
     uint32_t base = blockIdx.x * BS;
@@ -210,7 +210,7 @@ struct Eng {
   // The same with two entries per thread, i and i + half (half = ceil(cnt/2)),
   // so f gets two independent vertices whose dependent loads can overlap.
   template <class L, class F>
-  __device__ void for_list_pairs_pf(const uint32_t *lst, uint32_t cnt, L &&load, F &&f) {
+  __device__ __forceinline__ void for_list_pairs_pf(const uint32_t *lst, uint32_t cnt, L &&load, F &&f) {
     const uint32_t half = (cnt + 1u) / 2u;
     const uint32_t lim = (half + BS - 1u) / BS * BS;
     const uint32_t stride = gstride();
@@ -247,7 +247,7 @@ struct Eng {
   }
 
   template <class L, class F>
-  __device__ void for_vertices_pf(L &&load, F &&f) {
+  __device__ __forceinline__ void for_vertices_pf(L &&load, F &&f) {
     if (list_mode) {
       for_list_pf(P.s.act[act_sel], act_count, load, f);
       return;
@@ -276,60 +276,77 @@ struct Eng {
   // serialise every warp of the grid on one counter word in L2, and no CTA
   // barrier is involved (warps never wait for each other).
   struct Stage {
+    uint32_t n;      // items staged by this warp (identical in all 32 lanes)
+    uint32_t which;  // this warp's segment: stage_buf(which), stage_desc(which)
+  };
+  // Where a warp's segment drains to.  Kept in shared memory, not in the
+  // Stage: a sweep feeding two lists would otherwise hold six more
+  // registers per thread for values only a flush reads.
+  struct StageDesc {
     uint32_t *dst;
     uint32_t *count;
     uint32_t cap;
-    uint32_t n;     // items staged by this warp (identical in all 32 lanes)
-    uint32_t *buf;  // this warp's shared-memory segment (stage_buf)
   };
   static constexpr uint32_t kStage = BS >= 1024 ? 128 : 256;  // 2 segments per warp within 48 KB static
   // which = 0 or 1: two independent segments per warp (a sweep may feed two lists)
-  __device__ uint32_t *stage_buf(uint32_t which = 0) {
+  __device__ __forceinline__ uint32_t *stage_buf(uint32_t which = 0) {
     __shared__ uint32_t buf[2][BS / 32][kStage];
     return buf[which][threadIdx.x >> 5];
   }
-  __device__ void stage_flush(Stage &q) {
+  __device__ __forceinline__ StageDesc *stage_desc(uint32_t which) {
+    __shared__ StageDesc desc[2][BS / 32];
+    return &desc[which][threadIdx.x >> 5];
+  }
+  // all 32 lanes of the warp call it together
+  __device__ __forceinline__ Stage stage_open(uint32_t which, uint32_t *dst, uint32_t *count, uint32_t cap) {
+    if (lane_id() == 0) *stage_desc(which) = StageDesc{dst, count, cap};
     __syncwarp();
+    return Stage{0u, which};
+  }
+  __device__ __forceinline__ void stage_flush(Stage &q) {
+    __syncwarp();
+    const StageDesc d = *stage_desc(q.which);
     uint32_t base = 0;
-    if (lane_id() == 0 && q.n) base = atomicAdd(q.count, q.n);
+    if (lane_id() == 0 && q.n) base = atomicAdd(d.count, q.n);
     base = __shfl_sync(kFull, base, 0);
-    const uint32_t *buf = q.buf;
+    const uint32_t *buf = stage_buf(q.which);
     for (uint32_t i = lane_id(); i < q.n; i += 32) {
       const uint32_t pos = base + i;
-      if (pos < q.cap) q.dst[pos] = buf[i];
+      if (pos < d.cap) d.dst[pos] = buf[i];
       else atomicOr(err(), kErrQueueOverflow);
     }
     q.n = 0;
     __syncwarp();
   }
   // all 32 lanes of the warp call it together
-  __device__ void stage_put(Stage &q, bool pred, uint32_t v) {
+  __device__ __forceinline__ void stage_put(Stage &q, bool pred, uint32_t v) {
     const uint32_t mask = __ballot_sync(kFull, pred);
     if (!mask) return;
-    if (pred) q.buf[q.n + __popc(mask & lanemask_lt())] = v;
+    if (pred) stage_buf(q.which)[q.n + __popc(mask & lanemask_lt())] = v;
     q.n += __popc(mask);
     if (q.n > kStage - 32) stage_flush(q);
   }
   // every id 0 .. nwords*32-1 regardless of the active list
   template <class F>
-  __device__ void for_all_ids(F &&f) {
+  __device__ __forceinline__ void for_all_ids(F &&f) {
     const uint32_t lim = P.s.nwords * 32u;
     const uint32_t n = P.g.n;
     for (uint32_t v = gtid(); v < lim; v += gstride()) f(v, v >= 1 && v <= n);
   }
   // grid-stride over [0, cnt), whole CTAs
   template <class F>
-  __device__ void for_items(uint32_t cnt, F &&f) {
+  __device__ __forceinline__ void for_items(uint32_t cnt, F &&f) {
     const uint32_t lim = (cnt + BS - 1u) / BS * BS;
     for (uint32_t i = gtid(); i < lim; i += gstride()) f(i, i < cnt);
   }
 
-  __device__ bool live(uint32_t v) const { return !bit_test(P.s.elim, v); }
+  // Helpers below take the parameter blocks they read as arguments.
+  __device__ __forceinline__ static bool live(const EngState &s, uint32_t v) { return !bit_test(s.elim, v); }
 
-  __device__ uint32_t prio(uint32_t v) const {
-    if (P.o.pivot_rule == 0) return 0u;
-    const unsigned long long dout = ldg(P.g.off + v + 1) - ldg(P.g.off + v);
-    const unsigned long long din = ldg(P.g.offT + v + 1) - ldg(P.g.offT + v);
+  __device__ __forceinline__ static uint32_t prio(const EngGraph &g, uint32_t rule, uint32_t v) {
+    if (rule == 0) return 0u;
+    const unsigned long long dout = ldg(g.off + v + 1) - ldg(g.off + v);
+    const unsigned long long din = ldg(g.offT + v + 1) - ldg(g.offT + v);
     unsigned long long s = dout * din;
     if (s > 0xfffffffeull) s = 0xfffffffeull;
     return 0xfffffffeu - (uint32_t)s;
@@ -339,8 +356,8 @@ struct Eng {
   // scc_routines.cu:276-394: v is trimmed when it has no out-neighbour or no
   // in-neighbour that is not itself, not eliminated and (ranged) in its
   // partition.  Trimmed vertices become singleton SCCs (state 28).
-  __device__ bool live_nbr(const uint32_t *__restrict__ off, const uint32_t *__restrict__ adj, uint32_t v,
-                           uint32_t rv, bool ranged, bool snap) {
+  __device__ __forceinline__ static bool live_nbr(const EngState &s, const uint32_t *__restrict__ off, const uint32_t *__restrict__ adj,
+                                  uint32_t v, uint32_t rv, bool ranged, bool snap) {
     const uint32_t b = ldg(off + v), e = ldg(off + v + 1);
     if (snap) {  // nothing eliminated yet and lists sorted-unique
       const uint32_t d = e - b;
@@ -348,8 +365,8 @@ struct Eng {
     }
     for (uint32_t i = b; i < e; ++i) {
       const uint32_t u = ldg(adj + i);
-      if (u == v || !live(u)) continue;
-      if (ranged && ldm(P.s.range + u) != rv) continue;
+      if (u == v || !live(s, u)) continue;
+      if (ranged && ldm(s.range + u) != rv) continue;
       return true;
     }
     return false;
@@ -363,19 +380,25 @@ struct Eng {
   // The first trim sweep when nothing is eliminated yet and every list is
   // sorted-unique: only degrees decide (a list of one entry counts unless it
   // is a self-loop).  Each thread takes four consecutive ids with one 16-byte
-  // load of each offset array (the fifth offset comes from the next lane), so
-  // a warp covers four bitmap words per iteration; eliminated/trimmed words
-  // are assembled in registers.  Returns this thread's count of trimmed ids.
-  __device__ uint32_t trim_snap_sweep(bool pick, unsigned long long &best) {
+  // load of each offset array (the fifth offset comes from the next lane;
+  // lane 31 loads it), next iteration's loads in flight, so a warp covers
+  // four bitmap words per iteration and the sweep streams the offsets with
+  // no dependent load: an id whose decision needs the head of a single-entry
+  // list (the self-loop test) goes to its warp's shared-memory buffer, which
+  // the warp resolves in batches with all head loads in flight together.
+  // Eliminated/trimmed words are assembled in registers.  Returns this
+  // thread's count of trimmed ids.
+  __device__ __noinline__ uint32_t trim_snap_sweep(bool pick, unsigned long long &best) {
     const EngState &s = P.s;
     const EngGraph &g = P.g;
+    const uint32_t rule = P.o.pivot_rule;
     const uint32_t n = g.n;
     const uint32_t lim = s.nwords * 32u;  // multiple of 1024
     const uint32_t lane = lane_id();
     const bool vec = ((reinterpret_cast<uintptr_t>(g.off) | reinterpret_cast<uintptr_t>(g.offT)) & 15u) == 0;
     const uint32_t step = gstride() * 4u;
     struct Quad {
-      uint32_t o[4], t[4];
+      uint32_t o[4], t[4], o4, t4;
     };
     auto load = [&](uint32_t v0) {
       Quad q;
@@ -392,9 +415,56 @@ struct Eng {
           q.t[i] = in ? ldg(g.offT + v0 + i) : 0u;
         }
       }
+      const bool in4 = lane == 31 && v0 + 4u <= n + 1u;
+      q.o4 = in4 ? ldg(g.off + v0 + 4u) : 0u;
+      q.t4 = in4 ? ldg(g.offT + v0 + 4u) : 0u;
       return q;
     };
     uint32_t ntrim = 0;
+    // ids waiting for the self-loop test: this warp's stage segment
+    uint32_t *pend = stage_buf(0);
+    uint32_t npend = 0;  // warp-uniform
+    auto resolve = [&]() {
+      __syncwarp();
+      for (uint32_t i0 = 0; i0 < npend; i0 += 128u) {
+        uint32_t v[4], x[4], y[4];
+        bool ok[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const uint32_t i = i0 + j * 32u + lane;
+          ok[j] = i < npend;
+          v[j] = ok[j] ? pend[i] : 0u;
+        }
+        uint32_t ob[4], dout[4], tb[4], din[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          ob[j] = ok[j] ? ldg(g.off + v[j]) : 0u;
+          dout[j] = ok[j] ? ldg(g.off + v[j] + 1) - ob[j] : 0u;
+          tb[j] = ok[j] ? ldg(g.offT + v[j]) : 0u;
+          din[j] = ok[j] ? ldg(g.offT + v[j] + 1) - tb[j] : 0u;
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          x[j] = (ok[j] && dout[j] == 1) ? ldg(g.adj + ob[j]) : 0u;
+          y[j] = (ok[j] && din[j] == 1) ? ldg(g.adjT + tb[j]) : 0u;
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const bool tr = ok[j] && ((dout[j] == 1 && x[j] == v[j]) || (din[j] == 1 && y[j] == v[j]));
+          if (tr) {
+            s.label[v[j]] = v[j];
+            ++ntrim;
+          } else if (pick && ok[j]) {
+            const unsigned long long key = ((unsigned long long)prio(g, rule, v[j]) << 32) | v[j];
+            best = key < best ? key : best;
+          }
+          warp_set_bits(s.elim, v[j], tr, false);
+          warp_set_bits(s.tflag, v[j], tr, false);
+        }
+      }
+      npend = 0;
+      __syncwarp();
+    };
     uint32_t base = blockIdx.x * BS * 4u;
     const uint32_t wofs = (threadIdx.x >> 5) * 128u + lane * 4u;
     if (base >= lim) return 0;
@@ -406,35 +476,22 @@ struct Eng {
       if (base + step < lim) nxt = load(base + step + wofs);
       const Quad &q = cur_q;
       uint32_t o4 = __shfl_down_sync(kFull, q.o[0], 1), t4 = __shfl_down_sync(kFull, q.t[0], 1);
-      if (lane == 31) {
-        const bool in = v0 + 4u <= n + 1u;
-        o4 = in ? ldg(g.off + v0 + 4u) : 0u;
-        t4 = in ? ldg(g.offT + v0 + 4u) : 0u;
-      }
-      // degrees first; the single-entry lists' heads (self-loop test) are
-      // loaded together, and only where the other direction does not decide
-      uint32_t dout[4], din[4], x[4], y[4];
-#pragma unroll
-      for (int i = 0; i < 4; ++i) {
-        dout[i] = (i < 3 ? q.o[i + 1] : o4) - q.o[i];
-        din[i] = (i < 3 ? q.t[i + 1] : t4) - q.t[i];
-        const bool valid = v0 + i >= 1u && v0 + i <= n;
-        const bool open = valid && dout[i] != 0 && din[i] != 0;
-        x[i] = (open && dout[i] == 1) ? ldg(g.adj + q.o[i]) : 0u;
-        y[i] = (open && din[i] == 1) ? ldg(g.adjT + q.t[i]) : 0u;
-      }
-      uint32_t bits = 0;
+      if (lane == 31) o4 = q.o4, t4 = q.t4;
+      uint32_t bits = 0, amb = 0;
 #pragma unroll
       for (int i = 0; i < 4; ++i) {
         const uint32_t v = v0 + i;
+        const uint32_t dout = (i < 3 ? q.o[i + 1] : o4) - q.o[i];
+        const uint32_t din = (i < 3 ? q.t[i + 1] : t4) - q.t[i];
         if (v < 1u || v > n) continue;
-        const bool tr = dout[i] == 0 || din[i] == 0 || (dout[i] == 1 && x[i] == v) || (din[i] == 1 && y[i] == v);
-        if (tr) {
+        if (dout == 0 || din == 0) {
           s.label[v] = v;
           bits |= 1u << i;
           ++ntrim;
+        } else if (dout == 1 || din == 1) {
+          amb |= 1u << i;  // decided by the self-loop test
         } else if (pick) {
-          const unsigned long long key = ((unsigned long long)prio(v) << 32) | v;
+          const unsigned long long key = ((unsigned long long)prio(g, rule, v) << 32) | v;
           best = key < best ? key : best;
         }
       }
@@ -446,14 +503,26 @@ struct Eng {
         atomicOr(s.elim + w, word);
         atomicOr(s.tflag + w, word);
       }
+      // append this iteration's undecided ids (at most 128 per warp)
+      const uint32_t na = __popc(amb);
+      const uint32_t incl = warp_incl_scan(na);
+      const uint32_t tot = __shfl_sync(kFull, incl, 31);
+      if (npend + tot > kStage) resolve();
+      uint32_t at = npend + incl - na;
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+        if ((amb >> i) & 1u) pend[at++] = v0 + i;
+      npend += tot;
       cur_q = nxt;
     }
+    resolve();
     return ntrim;
   }
 
-  __device__ uint32_t trim(bool ranged, bool snap, uint32_t max_it, bool pick = false) {
+  __device__ __noinline__ uint32_t trim(bool ranged, bool snap, uint32_t max_it, bool pick = false) {
     const EngState &s = P.s;
     const EngGraph &g = P.g;
+    const uint32_t rule = P.o.pivot_rule;
     unsigned long long t0 = globaltimer_ns();
     uint32_t ntrim = 0;
     unsigned long long best = ~0ull;
@@ -468,7 +537,7 @@ struct Eng {
       prof(PR_TRIM_SWEEP, t0, 0);
       return 1;
     }
-    Stage tq{s.qa, cur() + C_Q, s.qcap, 0, stage_buf()};
+    Stage tq = stage_open(0, s.qa, cur() + C_Q, s.qcap);
     struct Pre {
       uint32_t ew, a0, a1, b0, b1;
     };
@@ -492,11 +561,11 @@ struct Eng {
           t = !(dout >= 2 || (dout == 1 && x != v)) || !(din >= 2 || (din == 1 && y != v));
         } else {
           const uint32_t rv = ranged ? ldm(s.range + v) : 0u;
-          t = !live_nbr(g.off, g.adj, v, rv, ranged, false) || !live_nbr(g.offT, g.adjT, v, rv, ranged, false);
+          t = !live_nbr(s, g.off, g.adj, v, rv, ranged, false) || !live_nbr(s, g.offT, g.adjT, v, rv, ranged, false);
         }
         if (t) s.label[v] = v;
         if (pick && !t) {
-          const unsigned long long key = ((unsigned long long)prio(v) << 32) | v;
+          const unsigned long long key = ((unsigned long long)prio(g, rule, v) << 32) | v;
           best = key < best ? key : best;
         }
       }
@@ -525,7 +594,7 @@ struct Eng {
         const uint32_t t = valid ? ldm(s.qa + i) : 0u;
         const uint32_t rt = (valid && ranged) ? ldm(s.range + t) : 0u;
         auto visit = [&](uint32_t, uint32_t u, uint32_t rtag) {
-          if (!live(u)) return;
+          if (!live(s, u)) return;
           if (ranged && ldm(s.range + u) != rtag) return;
           if (bit_claim(s.queued, u)) queue_push(s.qb, cur() + C_Q2, s.qcap, u, err());
         };
@@ -544,9 +613,9 @@ struct Eng {
         if (valid) {
           u = ldm(s.qb + i);
           bit_clear(s.queued, u);
-          if (live(u)) {
+          if (live(s, u)) {
             const uint32_t ru = ranged ? ldm(s.range + u) : 0u;
-            t = !live_nbr(g.off, g.adj, u, ru, ranged, false) || !live_nbr(g.offT, g.adjT, u, ru, ranged, false);
+            t = !live_nbr(s, g.off, g.adj, u, ru, ranged, false) || !live_nbr(s, g.offT, g.adjT, u, ru, ranged, false);
             if (t) s.label[u] = u;
           }
         }
@@ -568,11 +637,14 @@ struct Eng {
   // scc.cu:234-253: after the first trim the pivot is the first vertex that
   // is not eliminated (or, with SCC_PIVOT_MAX_DEGREE, the one with the
   // largest in x out degree).  Single partition only.
-  __device__ uint32_t pick_first_pivot() {
+  __device__ __noinline__ uint32_t pick_first_pivot() {
+    const EngState &s = P.s;
+    const EngGraph &g = P.g;
+    const uint32_t rule = P.o.pivot_rule;
     unsigned long long best = ~0ull;
     for_vertices([&](uint32_t v, bool valid) {
-      if (valid && live(v)) {
-        const unsigned long long key = ((unsigned long long)prio(v) << 32) | v;
+      if (valid && live(s, v)) {
+        const unsigned long long key = ((unsigned long long)prio(g, rule, v) << 32) | v;
         best = key < best ? key : best;
       }
     });
@@ -582,7 +654,7 @@ struct Eng {
     return commit_first_pivot();
   }
   // c->best holds the elected (priority, id) key; make it the pivot
-  __device__ uint32_t commit_first_pivot() {
+  __device__ __forceinline__ uint32_t commit_first_pivot() {
     const unsigned long long b = ldm64(&c->best);
     const uint32_t p = b == ~0ull ? 0u : (uint32_t)b;
     // c->best is reset by the lead after the next barrier (everyone has read it by then)
@@ -606,8 +678,10 @@ struct Eng {
   // live vertex moves to partition (range, F, B); one pivot per non-empty new
   // partition (smallest (priority, id)), which starts visited both ways.
   // Also used for the first election when the graph is segmented (F = B = 0).
-  __device__ void update() {
+  __device__ __noinline__ void update() {
     const EngState &s = P.s;
+    const EngGraph &g = P.g;
+    const uint32_t rule = P.o.pivot_rule;
     __shared__ uint32_t s_key[kSlotCache];
     __shared__ unsigned long long s_val[kSlotCache];
     __shared__ uint32_t s_szkey[kSizeCache], s_szcnt[kSizeCache];
@@ -653,13 +727,13 @@ struct Eng {
           nfound += p == v;  // one SCC per eliminated pivot
         } else {
           key = 3u * r + (f ? 1u : 0u) + (b ? 2u : 0u);
-          val = ((unsigned long long)prio(v) << 32) | v;
+          val = ((unsigned long long)prio(g, rule, v) << 32) | v;
         }
       }
       warp_set_bits(s.elim, v, fb, !list_mode);
       {  // SCC sizes: the warp's members of one component counted together
         const uint32_t pg = __match_any_sync(kFull, p);
-        if (fb && lane_id() == (uint32_t)(__ffs(pg) - 1)) size_add(s_szkey, s_szcnt, p, __popc(pg));
+        if (fb && lane_id() == (uint32_t)(__ffs(pg) - 1)) size_add(s, s_szkey, s_szcnt, p, __popc(pg));
       }
       const uint32_t grp = __match_any_sync(kFull, key);
       if (key != kNone) {
@@ -685,7 +759,7 @@ struct Eng {
       if (key != kNone && ldm64(s.slot + key) > s_val[i]) atomicMin(s.slot + key, s_val[i]);
     }
     for (int i = threadIdx.x; i < kSizeCache; i += BS)
-      if (s_szkey[i] != kNone) size_flush(s_szkey[i], s_szcnt[i]);
+      if (s_szkey[i] != kNone) size_flush(s, s_szkey[i], s_szcnt[i]);
     add_count(&c->n_fbe, nelim);
     add_count(&c->n_fbscc, nfound);
     if (!bar(300)) return;
@@ -754,7 +828,7 @@ struct Eng {
 
   // scc_routines.cu:10-19 unsetPivots: the pivots of the last election stop
   // being pivots (their visit bits go), used right before WCC.
-  __device__ void unset_pivots() {
+  __device__ __forceinline__ void unset_pivots() {
     const EngState &s = P.s;
     for (uint32_t w = gtid(); w < s.nwords; w += gstride()) {
       s.fvis[w] = 0u;
@@ -770,12 +844,12 @@ struct Eng {
   // Visit predicate shared by every arm: u joins the visited set of the
   // current direction when it is live, in the source's partition (unless
   // first step) and not visited yet; exactly one caller wins the claim.
-  __device__ bool try_visit(uint32_t *vis, uint32_t u, bool ranged, uint32_t rsrc) {
+  __device__ __forceinline__ static bool try_visit(const EngState &s, uint32_t *vis, uint32_t u, bool ranged, uint32_t rsrc) {
     const uint32_t w = u >> 5, b = 1u << (u & 31u);
-    const uint32_t vw = ldm(vis + w);        // both bitmap words are requested
-    const uint32_t ew = ldm(P.s.elim + w);   // before either is tested
+    const uint32_t vw = ldm(vis + w);      // both bitmap words are requested
+    const uint32_t ew = ldm(s.elim + w);   // before either is tested
     if ((vw | ew) & b) return false;
-    if (ranged && ldm(P.s.range + u) != rsrc) return false;
+    if (ranged && ldm(s.range + u) != rsrc) return false;
     return !(atomicOr(vis + w, b) & b);
   }
 
@@ -783,9 +857,12 @@ struct Eng {
   // four entries at a time (one 16-byte load once aligned) and the four
   // bitmap words are requested together, so a thread keeps several
   // independent L2 requests in flight instead of one dependent chain.
-  __device__ bool any_visited(const uint32_t *__restrict__ adj, uint32_t b, uint32_t e, const uint32_t *vis,
-                              bool ranged, uint32_t rv) {
-    const uint32_t *rng = P.s.range;
+  // wide: eight probes per step on unranged tests (more loads in flight per
+  // thread, but up to seven wasted bitmap lines when an early entry hits;
+  // callers that keep many candidates in flight pass false)
+  __device__ __forceinline__ static bool any_visited(const EngState &s, uint32_t m, const uint32_t *__restrict__ adj, uint32_t b,
+                                     uint32_t e, const uint32_t *vis, bool ranged, uint32_t rv, bool wide = true) {
+    const uint32_t *rng = s.range;
     auto hit = [&](uint32_t u) {
       return ((ldm(vis + (u >> 5)) >> (u & 31u)) & 1u) && (!ranged || ldm(rng + u) == rv);
     };
@@ -797,7 +874,7 @@ struct Eng {
       // the aligned 16 bytes holding the list head (entries of the previous
       // list masked off) instead of up to three dependent scalar probes
       const uint32_t a = i & ~3u;
-      if ((unsigned long long)a + 4ull <= P.g.m) {
+      if ((unsigned long long)a + 4ull <= m) {
         const uint4 q = __ldg(reinterpret_cast<const uint4 *>(adj + a));
         const uint32_t u[4] = {q.x, q.y, q.z, q.w};
         uint32_t w[4];
@@ -814,7 +891,7 @@ struct Eng {
         }
       }
     }
-    if (!ranged) {  // eight probes in flight per step
+    if (!ranged && wide) {  // eight probes in flight per step
       for (; vec && i + 8 <= e; i += 8) {
         const uint4 q = __ldg(reinterpret_cast<const uint4 *>(adj + i));
         const uint4 r = __ldg(reinterpret_cast<const uint4 *>(adj + i + 4));
@@ -849,14 +926,15 @@ struct Eng {
 
   // QUADRATIC (reach_q.cu:12-79,160-231): every sweep expands each visited,
   // not yet expanded vertex, one thread per vertex.
-  __device__ uint32_t reach_q(const uint32_t *__restrict__ off, const uint32_t *__restrict__ adj, uint32_t *vis,
+  __device__ __noinline__ uint32_t reach_q(const uint32_t *__restrict__ off, const uint32_t *__restrict__ adj, uint32_t *vis,
                               uint32_t *exp, bool ranged) {
+    const EngState &s = P.s;
     const uint32_t heavy = P.o.heavy_degree;
     uint32_t depth = 0;
     for (;;) {
       const unsigned long long ts = globaltimer_ns();
       uint32_t chg = 0;
-      auto visit = [&](uint32_t, uint32_t u, uint32_t rsrc) { chg += try_visit(vis, u, ranged, rsrc); };
+      auto visit = [&](uint32_t, uint32_t u, uint32_t rsrc) { chg += try_visit(s, vis, u, ranged, rsrc); };
       for_vertices([&](uint32_t v, bool valid) {
         // No warp-level "skip this word" shortcut here: visit bits change
         // under other warps during the sweep, so such a test would not be
@@ -864,15 +942,15 @@ struct Eng {
         // walked by the whole warp (warp_gather); a list longer than
         // heavy_degree goes to the grid (one hub's list would otherwise keep
         // a single thread busy for the whole sweep).
-        const bool fr = valid && live(v) && bit_test(vis, v) && !bit_test(exp, v);
+        const bool fr = valid && live(s, v) && bit_test(vis, v) && !bit_test(exp, v);
         warp_set_bits(exp, v, fr, !list_mode);
         uint32_t b = 0, d = 0, rv = 0;
         if (fr) {
-          rv = ranged ? ldm(P.s.range + v) : 0u;
+          rv = ranged ? ldm(s.range + v) : 0u;
           b = ldg(off + v);
           d = ldg(off + v + 1) - b;
           if (d > heavy) {
-            heavy_push(v, b, d, rv);
+            heavy_push(s, v, b, d, rv);
             d = 0;
           }
         }
@@ -884,7 +962,7 @@ struct Eng {
       if ((uint32_t)(h >> 32) != 0) {
         if (is_lead()) atomicAdd(cur() + C_CHG, rdprv(C_CHG));
         chg = 0;
-        heavy_expand(adj, h, visit);
+        heavy_expand(s, adj, h, visit);
         add_count(cur() + C_CHG, chg);
         if (!bar(501)) return depth;
       }
@@ -901,27 +979,27 @@ struct Eng {
 
   // Edges of lists longer than heavy_degree, collected during a push sweep
   // and expanded afterwards by the whole grid in 256-edge chunks.
-  __device__ void heavy_push(uint32_t v, uint32_t beg, uint32_t deg, uint32_t tag) {
+  __device__ __forceinline__ void heavy_push(const EngState &s, uint32_t v, uint32_t beg, uint32_t deg, uint32_t tag) {
     const unsigned long long old = atomicAdd(cur64(), (1ull << 32) | deg);
     const uint32_t idx = (uint32_t)(old >> 32);
-    if (idx >= P.s.hcap) {
+    if (idx >= s.hcap) {
       fail(kErrQueueOverflow);
       return;
     }
-    P.s.hv[idx] = v;
-    P.s.hbeg[idx] = beg;
-    P.s.hdeg[idx] = deg;
-    P.s.htag[idx] = tag;
-    P.s.hbase[idx] = (uint32_t)old;
+    s.hv[idx] = v;
+    s.hbeg[idx] = beg;
+    s.hdeg[idx] = deg;
+    s.htag[idx] = tag;
+    s.hbase[idx] = (uint32_t)old;
   }
 
   // heavy_expand for whole-warp visitors: visit(src, dst, tag, valid) on all
   // lanes at every step (valid = false past the end).
   template <class Visit>
-  __device__ void heavy_expand_all(const uint32_t *__restrict__ adj, unsigned long long h, Visit &&visit) {
+  __device__ __forceinline__ void heavy_expand_all(const EngState &s, const uint32_t *__restrict__ adj, unsigned long long h,
+                                   Visit &&visit) {
     const uint32_t cnt = (uint32_t)(h >> 32), tot = (uint32_t)h;
-    if (cnt == 0 || cnt > P.s.hcap) return;  // overflow already flagged by heavy_push
-    const EngState &s = P.s;
+    if (cnt == 0 || cnt > s.hcap) return;  // overflow already flagged by heavy_push
     const uint32_t lane = lane_id();
     for (uint32_t chunk = gwarp(); (unsigned long long)chunk * 256ull < tot; chunk += nwarps()) {
       const uint32_t e0 = chunk * 256u;
@@ -954,10 +1032,10 @@ struct Eng {
   }
 
   template <class Visit>
-  __device__ void heavy_expand(const uint32_t *__restrict__ adj, unsigned long long h, Visit &&visit) {
+  __device__ __forceinline__ void heavy_expand(const EngState &s, const uint32_t *__restrict__ adj, unsigned long long h,
+                               Visit &&visit) {
     const uint32_t cnt = (uint32_t)(h >> 32), tot = (uint32_t)h;
-    if (cnt == 0 || cnt > P.s.hcap) return;  // overflow already flagged by heavy_push
-    const EngState &s = P.s;
+    if (cnt == 0 || cnt > s.hcap) return;  // overflow already flagged by heavy_push
     const uint32_t lane = lane_id();
     for (uint32_t chunk = gwarp(); (unsigned long long)chunk * 256ull < tot; chunk += nwarps()) {
       const uint32_t e0 = chunk * 256u;
@@ -985,18 +1063,6 @@ struct Eng {
     }
   }
 
-  // Worklist reach: DATA / LINEAR / TOPO / BEST.  Levels are synchronous:
-  // level k expands the vertices first reached in level k-1 (the pivots at
-  // k = 0) and appends each vertex it reaches, exactly once, to the next
-  // worklist, so the n-slot worklists cannot overflow (reference
-  // worklistc.h:79-81 drops items instead).  DATA expands one item per
-  // thread (reach_d.cu); LINEAR gathers a level's edges warp-wide and splits
-  // heavy lists across the grid (reach_l.cu).  TOPO / BEST add the bottom-up
-  // topology sweep (reach_t.cu sweeps every vertex each level; reach_b.cu
-  // switches direction): when the frontier's edges exceed the unexplored
-  // edges / alpha, a level becomes a pull sweep -- every live unvisited
-  // vertex scans its reverse list for a visited partition-mate -- until fewer
-  // than live / beta vertices are reached per sweep.
   // Push levels run by CTA 0 alone while the frontier stays small (high-
   // diameter graphs spend hundreds of levels on a few dozen vertices each,
   // where a grid barrier per level costs more than the level).  Same visit
@@ -1004,7 +1070,7 @@ struct Eng {
   // through a shared-memory counter.  Results land in the counters C_L*.
   // The frontier's edges are checked first: too many and nothing is done
   // (C_LREF = 1), the grid expands that level instead.
-  __device__ void local_levels(const uint32_t *__restrict__ off, const uint32_t *__restrict__ adj, uint32_t *vis,
+  __device__ __noinline__ void local_levels(const uint32_t *__restrict__ off, const uint32_t *__restrict__ adj, uint32_t *vis,
                                bool ranged, const uint32_t *in, uint32_t nin, uint32_t sel, uint32_t max_levels) {
     const EngState &s = P.s;
     __shared__ uint32_t s_cnt, s_deg;
@@ -1033,7 +1099,7 @@ struct Eng {
       __syncthreads();
       uint32_t degsum = 0;
       auto visit = [&](uint32_t, uint32_t u, uint32_t rsrc) {
-        if (try_visit(vis, u, ranged, rsrc)) {
+        if (try_visit(s, vis, u, ranged, rsrc)) {
           const uint32_t pos = atomicAdd(&s_cnt, 1u);
           if (pos < s.qcap) lout[pos] = u;
           else fail(kErrQueueOverflow);
@@ -1074,11 +1140,208 @@ struct Eng {
     }
   }
 
+  // One pull sweep: every candidate (the vertices of `lst[0, lcnt)`, or
+  // every id when lst is null) that is live and not yet visited looks for a
+  // visited partition-mate among its reverse neighbours (poff / padj).  Found
+  // vertices are marked visited and appended to `out` (counter cur()[C_Q]);
+  // candidates not found go to `rem_out` (cur()[C_REM]); the found vertices'
+  // reverse degrees are summed into cur()[C_DEG].  Runs as its own function
+  // so the level driver's state does not take registers from the sweep.
+  template <bool ranged>
+  __device__ __noinline__ void pull_sweep(const uint32_t *__restrict__ poff, const uint32_t *__restrict__ padj,
+                                          uint32_t *vis, const uint32_t *lst, uint32_t lcnt, uint32_t *out,
+                                          uint32_t *rem_out, bool head_only) {
+    const EngState &s = P.s;
+    uint32_t degsum = 0;
+    Stage pq = stage_open(0, out, cur() + C_Q, s.qcap);
+    Stage rq = stage_open(1, rem_out, cur() + C_REM, s.qcap);
+    struct Pre {
+      uint32_t vw, ew, pb, pe, rv;
+    };
+    // Only v's own lane sets v's visit bit during a pull sweep, so the
+    // prefetched word is current for the bit this lane tests.  The
+    // frontier's edge count (for the direction heuristics) is taken from
+    // the reverse lists already loaded: in-degree stands in for
+    // out-degree, saving a random read of the other offsets per vertex.
+    auto load = [&](uint32_t v, bool valid) {
+      const uint32_t w = v >> 5, vv = valid ? v : 0u;
+      return Pre{ldm(vis + w), ldm(s.elim + w), ldg(poff + vv), ldg(poff + vv + 1),
+                 ranged ? ldm(s.range + vv) : 0u};
+    };
+    // Every lane's test starts with the aligned 16 bytes holding its list
+    // head; only entries of the list itself are probed (those 16 bytes
+    // also hold entries of the neighbouring lists, and these sweeps pay
+    // per distinct cache line their scattered loads touch).
+    const bool vec = (reinterpret_cast<uintptr_t>(padj) & 15u) == 0;
+    const uint32_t m = P.g.m;
+    auto head = [&](const Pre &p, bool cand, uint4 &q) {
+      const uint32_t a = p.pb & ~3u;  // a <= pb < pe <= m: m - a does not wrap
+      const bool h = vec && cand && p.pe > p.pb && m - a >= 4u;
+      q = h ? __ldg(reinterpret_cast<const uint4 *>(padj + a)) : make_uint4(0u, 0u, 0u, 0u);
+      return h;
+    };
+    auto probe_head = [&](const Pre &p, const uint4 &q, bool h, uint32_t (&w)[4]) {
+      const uint32_t a = p.pb & ~3u;
+      const uint32_t u[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+      for (int j = 0; j < 4; ++j) w[j] = (h && a + j >= p.pb && a + j < p.pe) ? ldm(vis + (u[j] >> 5)) : 0u;
+    };
+    auto head_hit = [&](const Pre &p, const uint4 &q, const uint32_t (&w)[4]) {
+      const uint32_t a = p.pb & ~3u;
+      const uint32_t u[4] = {q.x, q.y, q.z, q.w};
+      bool hit = false;
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+        if (a + j >= p.pb && a + j < p.pe && ((w[j] >> (u[j] & 31u)) & 1u) && (!ranged || ldm(s.range + u[j]) == p.rv))
+          hit = true;
+      return hit;
+    };
+    // rest of the list after the head: not in a heads-only sweep (unless
+    // the head could not be read, e.g. unaligned adjacency)
+    auto rest = [&](const Pre &p, bool cand, bool h) {
+      if (!cand || (head_only && h)) return false;
+      return any_visited(s, m, padj, h ? (p.pb & ~3u) + 4u : p.pb, p.pe, vis, ranged, p.rv, false);
+    };
+    if (lst) {
+      // two vertices per thread: both heads' loads, then both heads'
+      // probes, are issued together
+      for_list_pairs_pf(lst, lcnt, load,
+                        [&](uint32_t va, bool vla, const Pre &pa, uint32_t vb, bool vlb, const Pre &pb) {
+                          const bool ca = vla && !(((pa.vw | pa.ew) >> (va & 31u)) & 1u);
+                          const bool cb = vlb && !(((pb.vw | pb.ew) >> (vb & 31u)) & 1u);
+                          uint4 qa, qb;
+                          const bool ha = head(pa, ca, qa), hb = head(pb, cb, qb);
+                          uint32_t wa[4], wb[4];
+                          probe_head(pa, qa, ha, wa);
+                          probe_head(pb, qb, hb, wb);
+                          bool fa = ha && head_hit(pa, qa, wa);
+                          bool fb = hb && head_hit(pb, qb, wb);
+                          if (!fa) fa = rest(pa, ca, ha);
+                          if (!fb) fb = rest(pb, cb, hb);
+                          if (fa) degsum += pa.pe - pa.pb;
+                          if (fb) degsum += pb.pe - pb.pb;
+                          warp_set_bits(vis, va, fa, false);
+                          warp_set_bits(vis, vb, fb, false);
+                          stage_put(pq, fa, va);
+                          stage_put(pq, fb, vb);
+                          stage_put(rq, ca && !fa, va);
+                          stage_put(rq, cb && !fb, vb);
+                        });
+    } else {
+      // every id; a warp covers one bitmap word and skips words without a
+      // live unvisited vertex
+      for_vertices_pf(load, [&](uint32_t v, bool valid, const Pre &p) {
+        if ((~p.vw & ~p.ew) == 0u) return;
+        const bool cand = valid && !(((p.vw | p.ew) >> (v & 31u)) & 1u);
+        uint4 q;
+        uint32_t w[4];
+        const bool h = head(p, cand, q);
+        probe_head(p, q, h, w);
+        bool found = h && head_hit(p, q, w);
+        if (!found) found = rest(p, cand, h);
+        if (found) degsum += p.pe - p.pb;
+        warp_set_bits(vis, v, found, true);
+        stage_put(pq, found, v);
+        stage_put(rq, cand && !found, v);
+      });
+    }
+    stage_flush(pq);
+    stage_flush(rq);
+    add_count(cur() + C_DEG, degsum);
+  }
+
+  // One push level of the LINEAR / TOPO / BEST arms: the frontier in[0, nin)
+  // expands its lists warp-wide; newly reached vertices are appended to
+  // `out` through warp-staged segments (one global atomic per 224 items).
+  // Lists longer than `split` go to the grid-wide heavy list, expanded after
+  // a barrier in 256-edge chunks.  Returns false if a barrier failed; qoff
+  // receives the items the first interval appended (the heavy interval's
+  // count is in prv()[C_Q]); C_DEG sums the reached vertices' out-degrees
+  // when count_deg.
+  __device__ __noinline__ bool push_level(const uint32_t *__restrict__ off, const uint32_t *__restrict__ adj,
+                                          uint32_t *vis, bool ranged, bool count_deg, const uint32_t *in,
+                                          uint32_t nin, uint32_t *out, uint32_t split, uint32_t &qoff) {
+    const EngState &s = P.s;
+    uint32_t degsum = 0;
+    qoff = 0;
+    auto claim = [&](uint32_t u, uint32_t rsrc, bool valid) {
+      const bool claimed = valid && try_visit(s, vis, u, ranged, rsrc);
+      if (claimed && count_deg) degsum += ldg(off + u + 1) - ldg(off + u);
+      return claimed;
+    };
+    {
+      Stage fq = stage_open(0, out, cur() + C_Q, s.qcap);
+      auto visit_all = [&](uint32_t, uint32_t u, uint32_t rsrc, bool valid) { stage_put(fq, claim(u, rsrc, valid), u); };
+      for_items(nin, [&](uint32_t i, bool valid) {
+        uint32_t v = 0, b = 0, d = 0, rv = 0;
+        if (valid) {
+          v = ldm(in + i);
+          b = ldg(off + v);
+          d = ldg(off + v + 1) - b;
+          rv = ranged ? ldm(s.range + v) : 0u;
+          if (d > split) {
+            heavy_push(s, v, b, d, rv);
+            d = 0;
+          }
+        }
+        warp_gather_all(v, b, d, rv, adj, visit_all);
+      });
+      stage_flush(fq);
+    }
+    add_count(cur() + C_DEG, degsum);
+    if (!bar(700)) return false;
+    const unsigned long long h = ldm64(prv64());
+    if ((uint32_t)(h >> 32) != 0) {
+      const unsigned long long th = globaltimer_ns();
+      qoff = rdprv(C_Q);
+      if (is_lead()) atomicAdd(cur() + C_DEG, rdprv(C_DEG));
+      degsum = 0;
+      Stage hq = stage_open(0, out + qoff, cur() + C_Q, s.qcap - qoff);
+      heavy_expand_all(s, adj, h, [&](uint32_t, uint32_t u, uint32_t rsrc, bool valid) {
+        stage_put(hq, claim(u, rsrc, valid), u);
+      });
+      stage_flush(hq);
+      add_count(cur() + C_DEG, degsum);
+      if (!bar(701)) return false;
+      prof(PR_HEAVY, th, (uint32_t)(h >> 32), (uint32_t)h);
+    }
+    return true;
+  }
+
+  // One level of the DATA arm (reach_d.cu): a thread per frontier item walks
+  // its list alone.
+  __device__ __noinline__ void data_level(const uint32_t *__restrict__ off, const uint32_t *__restrict__ adj,
+                                          uint32_t *vis, bool ranged, const uint32_t *in, uint32_t nin,
+                                          uint32_t *out) {
+    const EngState &s = P.s;
+    uint32_t *cnt = cur() + C_Q;
+    for (uint32_t i = gtid(); i < nin; i += gstride()) {
+      const uint32_t v = ldm(in + i);
+      const uint32_t rv = ranged ? ldm(s.range + v) : 0u;
+      const uint32_t b = ldg(off + v), e = ldg(off + v + 1);
+      for (uint32_t j = b; j < e; ++j) {
+        const uint32_t u = ldg(adj + j);
+        if (try_visit(s, vis, u, ranged, rv)) queue_push(out, cnt, s.qcap, u, err());
+      }
+    }
+  }
+
+  // Worklist reach: DATA / LINEAR / TOPO / BEST.  Levels are synchronous:
+  // level k expands the vertices first reached in level k-1 (the pivots at
+  // k = 0) and appends each vertex it reaches, exactly once, to the next
+  // worklist, so the n-slot worklists cannot overflow (reference
+  // worklistc.h:79-81 drops items instead).  DATA expands one item per
+  // thread (reach_d.cu); LINEAR gathers a level's edges warp-wide and splits
+  // heavy lists across the grid (reach_l.cu).  TOPO / BEST add the bottom-up
+  // topology sweep (reach_t.cu sweeps every vertex each level; reach_b.cu
+  // switches direction): when the frontier's edges exceed the unexplored
+  // edges / alpha, a level becomes a pull sweep -- every live unvisited
+  // vertex scans its reverse list for a visited partition-mate -- until fewer
+  // than live / beta vertices are reached per sweep.
   __device__ uint32_t reach_wl(const uint32_t *__restrict__ off, const uint32_t *__restrict__ adj,
                                const uint32_t *__restrict__ poff, const uint32_t *__restrict__ padj, uint32_t *vis,
                                bool ranged, bool balanced, bool allow_pull) {
     const EngState &s = P.s;
-    const uint32_t heavy = P.o.heavy_degree;
     const long long alpha = P.o.pull_alpha > 0 ? P.o.pull_alpha : 14;
     const long long beta = P.o.pull_beta > 0 ? P.o.pull_beta : 24;
     const unsigned long long mtot = P.g.m;
@@ -1091,11 +1354,14 @@ struct Eng {
     const uint32_t *rem_in = nullptr;
     uint32_t rem_n = 0, rem_sel = 0;
     bool rem_valid = false;
-    while (nin > 0) {
+    // the last pull sweep tested list heads only: the next level must be a
+    // full pull sweep over the remaining list, even with an empty frontier
+    bool partial = false;
+    while (nin > 0 || partial) {
       const unsigned long long ts = globaltimer_ns();
       // a small frontier goes to CTA 0; if it refuses (too many edges), the
       // grid expands this level as usual and the next level tries again
-      if (!pull && nin <= kLocalMax) {
+      if (!pull && !partial && nin <= kLocalMax) {
         const uint32_t room = P.o.max_iters > depth ? P.o.max_iters - depth : 0u;
         if (blockIdx.x == 0) local_levels(off, adj, vis, ranged, in, nin, sel, room < kLocalLevels ? room : kLocalLevels);
         if (!bar(704)) return depth;
@@ -1116,179 +1382,56 @@ struct Eng {
           continue;
         }
       }
-      if (allow_pull) {
+      if (partial) {
+        pull = true;
+      } else if (allow_pull) {
         const unsigned long long unexplored = mtot > explored ? mtot - explored : 0ull;
         if (!pull && depth > 0 && (long long)mf * alpha > (long long)unexplored) pull = true;
         else if (pull && (long long)nin * beta < (long long)ldm(&c->n_live)) pull = false;
       }
       uint32_t *out = sel ? s.qb : s.qa;
-      uint32_t *cnt = cur() + C_Q;
       uint32_t qoff = 0;  // items already appended to `out` in an earlier interval of this level
-      uint32_t degsum = 0;
-      auto visit = [&](uint32_t, uint32_t u, uint32_t rsrc) {
-        if (try_visit(vis, u, ranged, rsrc)) {
-          queue_push(out + qoff, cnt, s.qcap - qoff, u, err());
-          if (allow_pull) degsum += ldg(off + u + 1) - ldg(off + u);
-        }
-      };
       uint32_t slot = PR_WL;
       if (pull) {
         slot = PR_PULL;
         if (is_lead()) atomicAdd(&c->pull_sweeps, 1u);
-        Stage pq{out, cnt, s.qcap, 0, stage_buf()};
-        struct Pre {
-          uint32_t vw, ew, pb, pe, rv;
-        };
-        // Only v's own lane sets v's visit bit during a pull sweep, so the
-        // prefetched word is current for the bit this lane tests.  The
-        // frontier's edge count (for the direction heuristics) is taken from
-        // the reverse lists already loaded: in-degree stands in for
-        // out-degree, saving a random read of the other offsets per vertex.
-        auto load = [&](uint32_t v, bool valid) {
-          const uint32_t w = v >> 5, vv = valid ? v : 0u;
-          return Pre{ldm(vis + w), ldm(s.elim + w), ldg(poff + vv), ldg(poff + vv + 1),
-                     ranged ? ldm(s.range + vv) : 0u};
-        };
         // Vertices a pull sweep examines but does not reach are kept in a
         // list, and the next pull sweep of this reach examines only them.
         uint32_t *rem_out = rem_sel ? s.pivkey : s.aux;
-        Stage rq{rem_out, cur() + C_REM, s.qcap, 0, stage_buf(1)};
-        auto body = [&](uint32_t v, bool valid, const Pre &p, bool aligned) {
-          // whole warp = one bitmap word in full mode: skip words without a live unvisited vertex
-          if (aligned && (~p.vw & ~p.ew) == 0u) return;
-          bool found = false;
-          const bool cand = valid && !(((p.vw | p.ew) >> (v & 31u)) & 1u);
-          if (cand) {
-            found = any_visited(padj, p.pb, p.pe, vis, ranged, p.rv);
-            if (found) degsum += p.pe - p.pb;
-          }
-          warp_set_bits(vis, v, found, aligned);
-          stage_put(pq, found, v);
-          stage_put(rq, cand && !found, v);
-        };
-        // List sweeps take two vertices per thread and probe the aligned 16
-        // bytes holding each list's head together (half of the candidates
-        // find a visited neighbour there); only those that do not go on to
-        // the rest of their list one at a time.
-        const bool vec = (reinterpret_cast<uintptr_t>(padj) & 15u) == 0;
-        auto head = [&](const Pre &p, bool cand, uint4 &q) {
-          const uint32_t a = p.pb & ~3u;
-          const bool h = vec && cand && p.pe > p.pb && (unsigned long long)a + 4ull <= P.g.m;
-          q = h ? __ldg(reinterpret_cast<const uint4 *>(padj + a)) : make_uint4(0u, 0u, 0u, 0u);
-          return h;
-        };
-        auto head_hit = [&](const Pre &p, const uint4 &q, const uint32_t (&w)[4]) {
-          const uint32_t a = p.pb & ~3u;
-          const uint32_t u[4] = {q.x, q.y, q.z, q.w};
-          bool hit = false;
-#pragma unroll
-          for (int j = 0; j < 4; ++j)
-            if (a + j >= p.pb && a + j < p.pe && ((w[j] >> (u[j] & 31u)) & 1u) &&
-                (!ranged || ldm(s.range + u[j]) == p.rv))
-              hit = true;
-          return hit;
-        };
-        auto pair_body = [&](uint32_t va, bool vla, const Pre &pa, uint32_t vb, bool vlb, const Pre &pb) {
-          const bool ca = vla && !(((pa.vw | pa.ew) >> (va & 31u)) & 1u);
-          const bool cb = vlb && !(((pb.vw | pb.ew) >> (vb & 31u)) & 1u);
-          uint4 qa, qb;
-          const bool ha = head(pa, ca, qa), hb = head(pb, cb, qb);
-          uint32_t wa[4], wb[4];
-          const uint32_t ua[4] = {qa.x, qa.y, qa.z, qa.w}, ub[4] = {qb.x, qb.y, qb.z, qb.w};
-#pragma unroll
-          for (int j = 0; j < 4; ++j) {
-            wa[j] = ha ? ldm(vis + (ua[j] >> 5)) : 0u;
-            wb[j] = hb ? ldm(vis + (ub[j] >> 5)) : 0u;
-          }
-          bool fa = ha && head_hit(pa, qa, wa);
-          bool fb = hb && head_hit(pb, qb, wb);
-          if (ca && !fa) fa = any_visited(padj, ha ? (pa.pb & ~3u) + 4u : pa.pb, pa.pe, vis, ranged, pa.rv);
-          if (cb && !fb) fb = any_visited(padj, hb ? (pb.pb & ~3u) + 4u : pb.pb, pb.pe, vis, ranged, pb.rv);
-          if (fa) degsum += pa.pe - pa.pb;
-          if (fb) degsum += pb.pe - pb.pb;
-          warp_set_bits(vis, va, fa, false);
-          warp_set_bits(vis, vb, fb, false);
-          stage_put(pq, fa, va);
-          stage_put(pq, fb, vb);
-          stage_put(rq, ca && !fa, va);
-          stage_put(rq, cb && !fb, vb);
-        };
-        if (rem_valid) {
-          for_list_pairs_pf(rem_in, rem_n, load, pair_body);
-        } else if (list_mode) {
-          for_list_pairs_pf(s.act[act_sel], act_count, load, pair_body);
-        } else {
-          for_vertices_pf(load, [&](uint32_t v, bool valid, const Pre &p) { body(v, valid, p, true); });
-        }
-        stage_flush(pq);
-        stage_flush(rq);
-        add_count(cur() + C_DEG, degsum);
+        const uint32_t *lst = rem_valid ? rem_in : list_mode ? s.act[act_sel] : nullptr;
+        const uint32_t lcnt = rem_valid ? rem_n : list_mode ? act_count : 0u;
+        // The first pull sweep after push levels covers every live vertex
+        // and most of them find a visited neighbour in their list head, so
+        // when the sweep set is large it tests heads only: a vertex whose
+        // head holds none goes to the remaining list unexamined beyond it,
+        // and the next sweep (forced to be a full pull sweep over that list)
+        // walks the rest.  Warps then no longer wait, iteration after
+        // iteration, for the few lanes walking long lists.
+        const uint32_t span = lst ? lcnt : P.g.n;
+        const bool head_only = (reinterpret_cast<uintptr_t>(padj) & 15u) == 0 && !rem_valid &&
+                               span >= 8u * gstride();
+        if (ranged) pull_sweep<true>(poff, padj, vis, lst, lcnt, out, rem_out, head_only);
+        else pull_sweep<false>(poff, padj, vis, lst, lcnt, out, rem_out, head_only);
         if (!bar(703)) return depth;
         rem_in = rem_out;
         rem_n = rdprv(C_REM);
         rem_valid = true;
         rem_sel ^= 1u;
+        partial = head_only;
       } else if (balanced) {
         rem_valid = false;
         // with a small frontier, lists longer than a chunk go to the whole grid
         // (one warp would otherwise walk thousands of edges while the rest wait)
         // (at most nwarps lists qualify, so the heavy-list counter sees few atomics);
         // mf (the frontier's edges) is known only where pulls are allowed
+        const uint32_t heavy = P.o.heavy_degree;
         const unsigned long long per_warp = mf / nwarps();
         uint32_t split = heavy;
         if (allow_pull && per_warp < heavy) split = per_warp < 256ull ? 256u : (uint32_t)per_warp;
-        // newly reached vertices go to the next frontier through warp-staged
-        // appends (one global atomic per 224 items, not per coalesced group)
-        auto claim = [&](uint32_t u, uint32_t rsrc, bool valid) {
-          const bool claimed = valid && try_visit(vis, u, ranged, rsrc);
-          if (claimed && allow_pull) degsum += ldg(off + u + 1) - ldg(off + u);
-          return claimed;
-        };
-        Stage fq{out, cnt, s.qcap, 0, stage_buf()};
-        auto visit_all = [&](uint32_t, uint32_t u, uint32_t rsrc, bool valid) {
-          stage_put(fq, claim(u, rsrc, valid), u);
-        };
-        for_items(nin, [&](uint32_t i, bool valid) {
-          uint32_t v = 0, b = 0, d = 0, rv = 0;
-          if (valid) {
-            v = ldm(in + i);
-            b = ldg(off + v);
-            d = ldg(off + v + 1) - b;
-            rv = ranged ? ldm(s.range + v) : 0u;
-            if (d > split) {
-              heavy_push(v, b, d, rv);
-              d = 0;
-            }
-          }
-          warp_gather_all(v, b, d, rv, adj, visit_all);
-        });
-        stage_flush(fq);
-        add_count(cur() + C_DEG, degsum);
-        if (!bar(700)) return depth;
-        const unsigned long long h = ldm64(prv64());
-        if ((uint32_t)(h >> 32) != 0) {
-          const unsigned long long th = globaltimer_ns();
-          qoff = rdprv(C_Q);
-          cnt = cur() + C_Q;
-          if (is_lead()) atomicAdd(cur() + C_DEG, rdprv(C_DEG));
-          degsum = 0;
-          Stage hq{out + qoff, cnt, s.qcap - qoff, 0, stage_buf()};
-          heavy_expand_all(adj, h, [&](uint32_t, uint32_t u, uint32_t rsrc, bool valid) {
-            stage_put(hq, claim(u, rsrc, valid), u);
-          });
-          stage_flush(hq);
-          add_count(cur() + C_DEG, degsum);
-          if (!bar(701)) return depth;
-          prof(PR_HEAVY, th, (uint32_t)(h >> 32), (uint32_t)h);
-        }
+        if (!push_level(off, adj, vis, ranged, allow_pull, in, nin, out, split, qoff)) return depth;
       } else {
-        for (uint32_t i = gtid(); i < nin; i += gstride()) {
-          const uint32_t v = ldm(in + i);
-          const uint32_t rv = ranged ? ldm(s.range + v) : 0u;
-          const uint32_t b = ldg(off + v), e = ldg(off + v + 1);
-          for (uint32_t j = b; j < e; ++j) visit(v, ldg(adj + j), rv);
-        }
-        add_count(cur() + C_DEG, degsum);
+        rem_valid = false;
+        data_level(off, adj, vis, ranged, in, nin, out);
         if (!bar(702)) return depth;
       }
       ++depth;
@@ -1328,41 +1471,41 @@ struct Eng {
   // representative (states 20 / 4).  Detection reads a snapshot (no
   // eliminations until every vertex has been examined), so the result does
   // not depend on thread order.
-  __device__ uint32_t single_live(const uint32_t *__restrict__ off, const uint32_t *__restrict__ adj, uint32_t v,
-                                  uint32_t rv) {
+  __device__ __forceinline__ static uint32_t single_live(const EngState &s, const uint32_t *__restrict__ off,
+                                         const uint32_t *__restrict__ adj, uint32_t v, uint32_t rv) {
     const uint32_t b = ldg(off + v), e = ldg(off + v + 1);
     uint32_t found = kNone, n = 0;
     for (uint32_t i = b; i < e; ++i) {
       const uint32_t u = ldg(adj + i);
-      if (u == v || !live(u) || ldm(P.s.range + u) != rv) continue;
+      if (u == v || !live(s, u) || ldm(s.range + u) != rv) continue;
       if (++n > 1) return kNone;
       found = u;
     }
     return found;
   }
-  __device__ bool only_to(const uint32_t *__restrict__ off, const uint32_t *__restrict__ adj, uint32_t u, uint32_t v,
-                          uint32_t rv) {
+  __device__ __forceinline__ static bool only_to(const EngState &s, const uint32_t *__restrict__ off, const uint32_t *__restrict__ adj,
+                                 uint32_t u, uint32_t v, uint32_t rv) {
     const uint32_t b = ldg(off + u), e = ldg(off + u + 1);
     uint32_t n = 0;
     for (uint32_t i = b; i < e; ++i) {
       const uint32_t w = ldg(adj + i);
-      if (w == u || !live(w) || ldm(P.s.range + w) != rv) continue;
+      if (w == u || !live(s, w) || ldm(s.range + w) != rv) continue;
       if (w != v) return false;
       ++n;
     }
     return n == 1;
   }
-  __device__ uint32_t trim2() {
+  __device__ __noinline__ uint32_t trim2() {
     const EngState &s = P.s;
     const EngGraph &g = P.g;
     for_vertices([&](uint32_t v, bool valid) {
-      if (!valid || !live(v)) return;
+      if (!valid || !live(s, v)) return;
       const uint32_t rv = ldm(s.range + v);
-      uint32_t u = single_live(g.off, g.adj, v, rv);
-      bool pair = u != kNone && only_to(g.off, g.adj, u, v, rv);
+      uint32_t u = single_live(s, g.off, g.adj, v, rv);
+      bool pair = u != kNone && only_to(s, g.off, g.adj, u, v, rv);
       if (!pair) {
-        u = single_live(g.offT, g.adjT, v, rv);
-        pair = u != kNone && only_to(g.offT, g.adjT, u, v, rv);
+        u = single_live(s, g.offT, g.adjT, v, rv);
+        pair = u != kNone && only_to(s, g.offT, g.adjT, u, v, rv);
       }
       if (pair) {
         s.aux[v] = u;
@@ -1396,13 +1539,13 @@ struct Eng {
   // they label, so updates may land in any order (atomicMin) and the fixpoint
   // is the same.  Lists are walked warp-wide, lists longer than heavy_degree
   // by the whole grid.
-  __device__ uint32_t wcc() {
+  __device__ __noinline__ uint32_t wcc() {
     const EngState &s = P.s;
     const EngGraph &g = P.g;
     const uint32_t heavy = P.o.heavy_degree;
     uint32_t *lab = s.aux;
     for_vertices([&](uint32_t v, bool valid) {
-      if (valid && live(v)) lab[v] = v;
+      if (valid && live(s, v)) lab[v] = v;
     });
     if (!bar(900)) return 0;
     uint32_t it = 0;
@@ -1410,19 +1553,19 @@ struct Eng {
       uint32_t chg = 0;
       // called from divergent code (warp_gather tails, heavy chunks): no warp collectives
       auto relax = [&](uint32_t src, uint32_t u, uint32_t rsrc) {
-        if (!live(u) || ldm(s.range + u) != rsrc) return;
+        if (!live(s, u) || ldm(s.range + u) != rsrc) return;
         const uint32_t x = ldm(lab + u);
         if (x < ldm(lab + src)) chg += atomicMin(lab + src, x) > x;
       };
       for_vertices([&](uint32_t v, bool valid) {
         uint32_t b = 0, d = 0, rv = 0;
-        const bool lv = valid && live(v);
+        const bool lv = valid && live(s, v);
         if (lv) {
           rv = ldm(s.range + v);
           b = ldg(g.off + v);
           d = ldg(g.off + v + 1) - b;
           if (d > heavy) {
-            heavy_push(v, b, d, rv);
+            heavy_push(s, v, b, d, rv);
             d = 0;
           }
         }
@@ -1438,7 +1581,7 @@ struct Eng {
       if ((uint32_t)(h >> 32) != 0) {
         if (is_lead()) atomicAdd(cur() + C_CHG, rdprv(C_CHG));
         chg = 0;
-        heavy_expand(g.adj, h, relax);
+        heavy_expand(s, g.adj, h, relax);
         add_count(cur() + C_CHG, chg);
         if (!bar(904)) return it;
       }
@@ -1452,7 +1595,7 @@ struct Eng {
     // roots become pivots of fresh partitions; members join their root's
     for_vertices([&](uint32_t v, bool valid) {
       bool root = false;
-      if (valid && live(v)) {
+      if (valid && live(s, v)) {
         const uint32_t r = ldm(lab + v);
         s.range[v] = r;
         root = r == v;
@@ -1478,7 +1621,7 @@ struct Eng {
   }
 
   // ============================================= active-list compaction
-  __device__ void compact() {
+  __device__ __noinline__ void compact() {
     const EngState &s = P.s;
     uint32_t *dst = s.act[act_sel ^ 1u];
     if (!list_mode) {
@@ -1508,7 +1651,7 @@ struct Eng {
         }
       }
     } else {
-      Stage aq{dst, cur() + C_Q, s.qcap, 0, stage_buf()};
+      Stage aq = stage_open(0, dst, cur() + C_Q, s.qcap);
       for_vertices_pf([&](uint32_t v, bool) { return ldm(s.elim + (v >> 5)); },
                       [&](uint32_t v, bool valid, uint32_t ew) {
                         stage_put(aq, valid && !((ew >> (v & 31u)) & 1u), v);
@@ -1526,13 +1669,13 @@ struct Eng {
   }
 
   // compacts when fewer than span * den / num vertices are live
-  __device__ void maybe_compact(uint32_t num = 4, uint32_t den = 1) {
+  __device__ __forceinline__ void maybe_compact(uint32_t num = 4, uint32_t den = 1) {
     const uint32_t nlive = ldm(&c->n_live);
     const uint32_t span = list_mode ? act_count : P.g.n;
     if (nlive > 0 && (unsigned long long)nlive * num < (unsigned long long)span * den) compact();
   }
 
-  __device__ void sync_live() {
+  __device__ __forceinline__ void sync_live() {
     // n_live = n - trimmed - trim2 - F∩B; every CTA computes the same value
     if (is_lead()) {
       const uint32_t gone = ldm(&c->n_trimmed) + ldm(&c->n_trim2) + ldm(&c->n_fbe);
@@ -1541,7 +1684,7 @@ struct Eng {
   }
 
   // ================================================== finalize labels
-  __device__ void finalize() {
+  __device__ __noinline__ void finalize() {
     const EngState &s = P.s;
     list_mode = 0;
     if (P.o.pivot_rule != 0) {  // representatives are pivots: canonicalise to min id
@@ -1577,11 +1720,11 @@ struct Eng {
   }
 
   // ================================================= the driver (a3)
-  __device__ void timed(unsigned long long &acc, unsigned long long t0) {
+  __device__ __forceinline__ void timed(unsigned long long &acc, unsigned long long t0) {
     if (is_lead()) acc += globaltimer_ns() - t0;
   }
 
-  __device__ uint32_t arm_for(bool below) const {
+  __device__ __forceinline__ uint32_t arm_for(bool below) const {
     switch (P.o.alg) {
       case 0: return ARM_Q;
       case 1: return ARM_T;
@@ -1733,6 +1876,8 @@ __global__ void __launch_bounds__(BS, MINB) scc_persistent(const __grid_constant
       const uint32_t it = e.trim(false, snap, p.o.max_iters);
       e.sync_live();
       if (e.is_lead()) c->phase_ret = it;
+      // as in the solve: later sweeps cover the survivors' list when few survive
+      if (e.bar(1)) e.maybe_compact(5, 4);
       break;
     }
     case PH_TRIM: {
