@@ -35,7 +35,7 @@ class scc_opts(C.Structure):
         ("switch_permille", C.c_int32), ("trim_depth", C.c_int32), ("pull_alpha", C.c_int32),
         ("pull_beta", C.c_int32), ("warp_degree", C.c_uint32), ("heavy_degree", C.c_uint32),
         ("max_iters", C.c_uint32), ("grid_blocks", C.c_uint32), ("timeout_ms", C.c_uint32),
-        ("trim_first_depth", C.c_int32), ("occupancy", C.c_int32),
+        ("trim_first_depth", C.c_int32), ("occupancy", C.c_int32), ("async_depth", C.c_int32),
         ("test_stall_us", C.c_uint32), ("test_queue_cap", C.c_uint32),
     ]
 

@@ -149,7 +149,8 @@ int ensure_state(scc_ctx *c) {
   CK(c->act1.ensure(vb), "alloc active list");
   CK(c->piv.ensure(vb), "alloc pivot list");
   CK(c->pivkey.ensure(vb), "alloc pivot keys");
-  const size_t slot_bytes = ((size_t)cn + 1) * 3 * 8;
+  // election slots, then the asynchronous reach queue: both all ones between uses
+  const size_t slot_bytes = ((size_t)cn + 1) * 3 * 8 + ((size_t)cn + 1) * 4;
   if (slot_bytes > c->slot.bytes) c->slot_dirty = true;
   CK(c->slot.ensure(slot_bytes), "alloc election slots");
   CK(c->heavy.ensure((size_t)ch * 5 * 4), "alloc heavy list");
@@ -198,6 +199,7 @@ sccb::Params make_params(scc_ctx *c, uint32_t *out_labels) {
   s.piv = c->piv.as<uint32_t>();
   s.pivkey = c->pivkey.as<uint32_t>();
   s.slot = c->slot.as<unsigned long long>();
+  s.aq = reinterpret_cast<uint32_t *>(s.slot + 3 * ((size_t)c->cap_n + 1));
   uint32_t *h = c->heavy.as<uint32_t>();
   s.hv = h;
   s.hbeg = h + (size_t)c->cap_h;
@@ -227,6 +229,7 @@ sccb::Params make_params(scc_ctx *c, uint32_t *out_labels) {
   e.max_iters = o.max_iters ? o.max_iters : (1u << 20);
   e.timeout_ns = (unsigned long long)(o.timeout_ms ? o.timeout_ms : 10000u) * 1000000ull;
   e.trim_first_depth = o.trim_first_depth;
+  e.async_depth = o.async_depth ? o.async_depth : 4;
   e.test_stall_ns = (unsigned long long)o.test_stall_us * 1000ull;
   // a test cap only shortens the usable part of the (n+1)-entry worklists
   if (o.test_queue_cap && o.test_queue_cap < s.qcap) s.qcap = o.test_queue_cap;

@@ -33,7 +33,17 @@ enum : uint32_t {
 // kLocalEdges edges are expanded by CTA 0 alone with CTA barriers, at most
 // kLocalLevels levels per grid barrier
 constexpr uint32_t kLocalMax = 2048, kLocalEdges = 4096, kLocalLevels = 4096;
-enum : uint32_t { ARM_Q = 0, ARM_T = 1, ARM_D = 2, ARM_L = 3, ARM_B = 6 };
+// push levels whose frontier has at most this many edges per vertex test
+// targets with try_visit_wide
+constexpr uint32_t kWideDegree = 16;
+// polls of a partly filled window before an asynchronous step expands it
+constexpr uint32_t kAsyncHold = 2;
+// graphs of at most this many vertices run on one CTA per SM by default
+constexpr uint32_t kSmallGraphN = 1u << 21;
+// HYBRID / COMBINE / BEST tails are asynchronous reaches on graphs of at most
+// this many edges per vertex
+constexpr uint32_t kAsyncTailDegree = 12;
+enum : uint32_t { ARM_Q = 0, ARM_T = 1, ARM_D = 2, ARM_L = 3, ARM_B = 6, ARM_TA = 7 };
 
 constexpr int kSlotCache = 128;  // per-CTA cache of partition-election slots
 constexpr int kSizeCache = 32;   // per-CTA cache of SCC-size counters
@@ -289,9 +299,13 @@ struct Eng {
   };
   static constexpr uint32_t kStage = BS >= 1024 ? 128 : 256;  // 2 segments per warp within 48 KB static
   // which = 0 or 1: two independent segments per warp (a sweep may feed two lists)
+  // the staging segments of all warps, 2 * (BS / 32) * kStage >= 8 * BS words
+  __device__ __forceinline__ uint32_t *stage_mem() {
+    __shared__ uint32_t buf[2 * (BS / 32) * kStage];
+    return buf;
+  }
   __device__ __forceinline__ uint32_t *stage_buf(uint32_t which = 0) {
-    __shared__ uint32_t buf[2][BS / 32][kStage];
-    return buf[which][threadIdx.x >> 5];
+    return stage_mem() + (which * (BS / 32) + (threadIdx.x >> 5)) * kStage;
   }
   __device__ __forceinline__ StageDesc *stage_desc(uint32_t which) {
     __shared__ StageDesc desc[2][BS / 32];
@@ -852,6 +866,20 @@ struct Eng {
     if (ranged && ldm(s.range + u) != rsrc) return false;
     return !(atomicOr(vis + w, b) & b);
   }
+  // try_visit that requests u's partition id and (want_deg) u's offsets
+  // together with the bitmap words: one round trip before the claim instead
+  // of up to three, for levels bound by latency rather than by bytes
+  __device__ __forceinline__ static bool try_visit_wide(const EngState &s, const uint32_t *__restrict__ off, uint32_t *vis,
+                                                        uint32_t u, bool ranged, uint32_t rsrc, bool want_deg,
+                                                        uint32_t &deg) {
+    const uint32_t w = u >> 5, b = 1u << (u & 31u);
+    const uint32_t vw = ldm(vis + w), ew = ldm(s.elim + w);
+    const uint32_t rg = ranged ? ldm(s.range + u) : rsrc;
+    const uint32_t o0 = want_deg ? ldg(off + u) : 0u, o1 = want_deg ? ldg(off + u + 1) : 0u;
+    deg = o1 - o0;
+    if (((vw | ew) & b) || rg != rsrc) return false;
+    return !(atomicOr(vis + w, b) & b);
+  }
 
   // Pull test: does adj[b, e) hold a visited partition-mate?  Lists are read
   // four entries at a time (one 16-byte load once aligned) and the four
@@ -1070,10 +1098,47 @@ struct Eng {
   // through a shared-memory counter.  Results land in the counters C_L*.
   // The frontier's edges are checked first: too many and nothing is done
   // (C_LREF = 1), the grid expands that level instead.
+  // CTA-wide exclusive scan of x (every thread calls); the total goes to `tot`.
+  __device__ __forceinline__ static uint32_t block_excl_scan(uint32_t x, uint32_t &tot) {
+    __shared__ uint32_t s_w[BS / 32 + 1];
+    const uint32_t lane = lane_id(), w = threadIdx.x >> 5;
+    const uint32_t incl = warp_incl_scan(x);
+    if (lane == 31) s_w[w] = incl;
+    __syncthreads();
+    if (w == 0) {
+      const uint32_t t = lane < BS / 32 ? s_w[lane] : 0u;
+      const uint32_t ti = warp_incl_scan(t);
+      if (lane < BS / 32) s_w[lane] = ti - t;
+      if (lane == 31) s_w[BS / 32] = ti;
+    }
+    __syncthreads();
+    tot = s_w[BS / 32];
+    const uint32_t r = s_w[w] + incl - x;
+    __syncthreads();
+    return r;
+  }
+
+  // Levels of a small frontier expanded by this CTA alone (CTA 0, between
+  // two grid barriers), CTA barriers between levels.  A level's edges are
+  // spread over all threads of the CTA, whatever the lists' lengths (a
+  // pivot's list of thousands of edges takes a few steps of the CTA, not
+  // thousands / 32 steps of one warp): the frontier is taken BS sources at a
+  // time, their degrees scanned into a shared-memory table, and every thread
+  // then takes edges e, e + BS, ... of the chunk, four per step, finding each
+  // edge's source by binary search in the table.  The bitmap words, the
+  // partition id and the offsets of the four targets are requested together,
+  // so a step costs three dependent round trips (list entry, tests, claim).
+  // Results for the level driver go to cur()[C_L*]; C_LREF = 1 when the
+  // frontier's edges exceed kLocalEdges (nothing done).
   __device__ __noinline__ void local_levels(const uint32_t *__restrict__ off, const uint32_t *__restrict__ adj, uint32_t *vis,
                                bool ranged, const uint32_t *in, uint32_t nin, uint32_t sel, uint32_t max_levels) {
     const EngState &s = P.s;
     __shared__ uint32_t s_cnt, s_deg;
+    // source table of the current chunk, in the staging segments (no stage
+    // is open in this CTA between the grid barriers around this call)
+    uint32_t *const s_base = stage_mem();  // adjacency index of a chunk edge = s_base[src] + edge
+    uint32_t *const s_ex = s_base + BS;    // first chunk edge of each source
+    uint32_t *const s_rv = s_base + 2 * BS;
     uint32_t d = 0;
     for (uint32_t i = threadIdx.x; i < nin; i += BS) {
       const uint32_t v = ldm(in + i);
@@ -1090,24 +1155,16 @@ struct Eng {
     }
     uint32_t lnin = nin, ld = 0, lsel = sel, lex = 0;
     const uint32_t *lin = in;
+    const uint32_t qcap = s.qcap;
     while (lnin > 0 && ld < max_levels) {
       uint32_t *lout = lsel ? s.qb : s.qa;
       if (threadIdx.x == 0) {
         s_cnt = 0;
         s_deg = 0;
       }
-      __syncthreads();
+      // (the scan's barriers order these writes before any use)
       uint32_t degsum = 0;
-      auto visit = [&](uint32_t, uint32_t u, uint32_t rsrc) {
-        if (try_visit(s, vis, u, ranged, rsrc)) {
-          const uint32_t pos = atomicAdd(&s_cnt, 1u);
-          if (pos < s.qcap) lout[pos] = u;
-          else fail(kErrQueueOverflow);
-          degsum += ldg(off + u + 1) - ldg(off + u);
-        }
-      };
-      const uint32_t lim = (lnin + BS - 1u) / BS * BS;
-      for (uint32_t base = 0; base < lim; base += BS) {
+      for (uint32_t base = 0; base < lnin; base += BS) {
         const uint32_t i = base + threadIdx.x;
         uint32_t v = 0, b = 0, dd = 0, rv = 0;
         if (i < lnin) {
@@ -1116,7 +1173,55 @@ struct Eng {
           dd = ldg(off + v + 1) - b;
           rv = ranged ? ldm(s.range + v) : 0u;
         }
-        warp_gather(v, b, dd, rv, adj, visit);
+        uint32_t tot;
+        const uint32_t ex = block_excl_scan(dd, tot);
+        s_base[threadIdx.x] = b - ex;
+        s_ex[threadIdx.x] = ex;
+        s_rv[threadIdx.x] = rv;
+        __syncthreads();
+        const uint32_t nsrc = lnin - base < (uint32_t)BS ? lnin - base : (uint32_t)BS;
+        for (uint32_t e0 = threadIdx.x; e0 < tot; e0 += 4u * BS) {
+          uint32_t u[4], r[4];
+          bool ok[4];
+#pragma unroll
+          for (int j = 0; j < 4; ++j) {
+            const uint32_t e = e0 + (uint32_t)j * BS;
+            ok[j] = e < tot;
+            // largest source index whose first edge is <= e (sources without
+            // edges share their successor's first edge and are skipped)
+            uint32_t lo = 0, hi = nsrc;
+            while (hi - lo > 1u) {
+              const uint32_t mid = (lo + hi) >> 1;
+              if (s_ex[mid] <= e) lo = mid;
+              else hi = mid;
+            }
+            // u32 sum first: s_base holds list start - first chunk edge, modulo 2^32
+            u[j] = ok[j] ? ldg(adj + (s_base[lo] + e)) : 0u;
+            r[j] = s_rv[lo];
+          }
+          uint32_t vw[4], ew[4], rg[4], o0[4], o1[4];
+#pragma unroll
+          for (int j = 0; j < 4; ++j) {
+            const uint32_t w = u[j] >> 5;
+            vw[j] = ok[j] ? ldm(vis + w) : ~0u;
+            ew[j] = ok[j] ? ldm(s.elim + w) : ~0u;
+            rg[j] = ok[j] && ranged ? ldm(s.range + u[j]) : 0u;
+            o0[j] = ok[j] ? ldg(off + u[j]) : 0u;
+            o1[j] = ok[j] ? ldg(off + u[j] + 1) : 0u;
+          }
+#pragma unroll
+          for (int j = 0; j < 4; ++j) {
+            const uint32_t bit = 1u << (u[j] & 31u);
+            const bool cand = !((vw[j] | ew[j]) & bit) && (!ranged || rg[j] == r[j]);
+            if (cand && !(atomicOr(vis + (u[j] >> 5), bit) & bit)) {
+              const uint32_t pos = atomicAdd(&s_cnt, 1u);
+              if (pos < qcap) lout[pos] = u[j];
+              else fail(kErrQueueOverflow);
+              degsum += o1[j] - o0[j];
+            }
+          }
+        }
+        __syncthreads();  // the table is rewritten by the next chunk
       }
       degsum = __reduce_add_sync(kFull, degsum);
       if (lane_id() == 0 && degsum) atomicAdd(&s_deg, degsum);
@@ -1260,11 +1365,20 @@ struct Eng {
   // when count_deg.
   __device__ __noinline__ bool push_level(const uint32_t *__restrict__ off, const uint32_t *__restrict__ adj,
                                           uint32_t *vis, bool ranged, bool count_deg, const uint32_t *in,
-                                          uint32_t nin, uint32_t *out, uint32_t split, uint32_t &qoff) {
+                                          uint32_t nin, uint32_t *out, uint32_t split, uint32_t &qoff, bool wide) {
     const EngState &s = P.s;
     uint32_t degsum = 0;
     qoff = 0;
+    // frontiers of short lists are latency-bound: their targets' tests and
+    // offsets are requested in one round trip (wide; for long lists the
+    // extra loads of targets already visited cost more than they save)
     auto claim = [&](uint32_t u, uint32_t rsrc, bool valid) {
+      if (wide) {
+        uint32_t dg = 0;
+        const bool claimed = valid && try_visit_wide(s, off, vis, u, ranged, rsrc, count_deg, dg);
+        if (claimed) degsum += dg;
+        return claimed;
+      }
       const bool claimed = valid && try_visit(s, vis, u, ranged, rsrc);
       if (claimed && count_deg) degsum += ldg(off + u + 1) - ldg(off + u);
       return claimed;
@@ -1326,6 +1440,177 @@ struct Eng {
     }
   }
 
+  // Asynchronous tail of a worklist reach (no levels).  A deep, thin reach
+  // (a grid's thousands of levels of a few thousand vertices) is bound by
+  // per-level latency -- a grid barrier plus the dependent loads of one
+  // expansion -- not by bytes.  Reachability does not need levels: the
+  // frontier in[0, nin) is copied into the queue aq, and from then on every
+  // warp repeatedly takes the next 32 slots (one atomicAdd on aq_head),
+  // expands the vertices of its slots as they are filled (the 32 lists
+  // walked as one concatenation, 128 edges per round of loads), and appends
+  // every vertex it claims (exactly once, through the visited bitmap) with
+  // one atomic per step on aq_td, which holds the slots appended (high
+  // half) and the vertices expanded (low half).  A consumed slot is reset to
+  // kNone, so aq is all ones again when the reach ends.  The reach is over
+  // when the two halves are equal: a step's appends are counted in the same
+  // atomic as its sources, so equal halves mean no expansion is in flight
+  // and none can start.  Filled slots never wait long behind unfilled ones
+  // of the same window (at most kAsyncHold polls).  Waits are bounded: no
+  // progress for timeout_ns sets kErrBarrierTimeout.
+  // Appends the k claims staged in stb (all 32 lanes call) and counts
+  // `done` expanded sources, with one atomic on aq_td (tail << 32 | done).
+  __device__ __forceinline__ void async_append(const uint32_t *stb, uint32_t k, uint32_t done) {
+    __syncwarp();
+    unsigned long long old = 0;
+    if (lane_id() == 0 && (k | done)) old = atomicAdd(&c->aq_td, ((unsigned long long)k << 32) | done);
+    const uint32_t pos = (uint32_t)(__shfl_sync(kFull, old, 0) >> 32);
+    for (uint32_t i = lane_id(); i < k; i += 32u) {
+      if (pos + i < P.s.qcap) P.s.aq[pos + i] = stb[i];
+      else fail(kErrQueueOverflow);
+    }
+    __syncwarp();
+  }
+
+  __device__ __noinline__ void async_reach(const uint32_t *__restrict__ off, const uint32_t *__restrict__ adj,
+                                           uint32_t *vis, bool ranged, const uint32_t *in, uint32_t nin) {
+    const EngState &s = P.s;
+    uint32_t *aq = s.aq;
+    const uint32_t qcap = s.qcap;
+    const uint32_t nseed = nin < qcap ? nin : qcap;
+    for_items(nseed, [&](uint32_t i, bool valid) {
+      if (valid) aq[i] = ldm(in + i);
+    });
+    if (is_lead()) {
+      if (nin > qcap) fail(kErrQueueOverflow);
+      c->aq_head = 0;
+      c->aq_td = (unsigned long long)nin << 32;
+    }
+    if (!bar(710)) return;
+    const uint32_t lane = lane_id();
+    uint32_t *const stb = stage_buf(0);  // this warp's claims of the current step
+    uint32_t steps = 0;  // warp steps (lane 0 counts them)
+    bool over = false;
+    while (!over) {
+      uint32_t base = 0;
+      if (lane == 0) base = atomicAdd(&c->aq_head, 32u);
+      base = __shfl_sync(kFull, base, 0);
+      if (base >= qcap) break;  // every slot is taken: nothing more can come this warp's way
+      const uint32_t slot = base + lane;
+      bool pend = slot < qcap;
+      unsigned long long idle0 = 0;
+      uint32_t nap = 32, idle = 0, hold = 0;
+      while (__any_sync(kFull, pend)) {
+        const uint32_t v = pend ? ldm(aq + slot) : kNone;
+        const bool rdy = pend && v != kNone;
+        const uint32_t rmask = __ballot_sync(kFull, rdy);
+        // a partly filled window is polled again once or twice before it is
+        // expanded: while the reach is wide its other slots fill within
+        // nanoseconds, and a step then expands up to 32 vertices, not two
+        if (rmask && rmask != __ballot_sync(kFull, pend) && hold < kAsyncHold) {
+          ++hold;
+          __nanosleep(32);
+          continue;
+        }
+        if (rmask) {
+          idle0 = 0;
+          nap = 32;
+          idle = 0;
+          hold = 0;
+          ++steps;
+          uint32_t b = 0, d = 0, rv = 0;
+          if (rdy) {
+            b = ldg(off + v);
+            d = ldg(off + v + 1) - b;
+            rv = ranged ? ldm(s.range + v) : 0u;
+            aq[slot] = kNone;
+          }
+          // the 32 lists walked as one concatenation, four 32-edge rounds
+          // at a time with each round's loads issued together; claimed
+          // vertices wait in this warp's staging segment
+          const uint32_t incl = warp_incl_scan(d);
+          const uint32_t total = __shfl_sync(kFull, incl, 31);
+          const uint32_t excl = incl - d;
+          uint32_t nst = 0;  // staged claims (warp-uniform)
+          for (uint32_t e0 = 0; e0 < total; e0 += 128u) {
+            uint32_t u[4], rs[4];
+            bool val[4];
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+              const uint32_t e = e0 + 32u * r + lane;
+              uint32_t lo = 0;  // owner: largest lane whose slice starts at or before e
+#pragma unroll
+              for (uint32_t sft = 16; sft >= 1; sft >>= 1) {
+                const uint32_t cand = lo + sft;
+                const uint32_t ex = __shfl_sync(kFull, excl, cand & 31u);
+                if (cand < 32 && ex <= e) lo = cand;
+              }
+              const uint32_t o_beg = __shfl_sync(kFull, b, lo), o_ex = __shfl_sync(kFull, excl, lo);
+              rs[r] = __shfl_sync(kFull, rv, lo);
+              val[r] = e < total;
+              u[r] = val[r] ? ldg(adj + o_beg + (e - o_ex)) : 0u;
+            }
+            uint32_t vw[4], ew[4], rg[4];
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+              vw[r] = val[r] ? ldm(vis + (u[r] >> 5)) : ~0u;
+              ew[r] = val[r] ? ldm(s.elim + (u[r] >> 5)) : ~0u;
+              rg[r] = val[r] && ranged ? ldm(s.range + u[r]) : rs[r];
+            }
+            bool cl[4];
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+              const uint32_t bit = 1u << (u[r] & 31u);
+              cl[r] = !((vw[r] | ew[r]) & bit) && rg[r] == rs[r] && !(atomicOr(vis + (u[r] >> 5), bit) & bit);
+            }
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+              const uint32_t m = __ballot_sync(kFull, cl[r]);
+              if (cl[r]) stb[nst + __popc(m & lanemask_lt())] = u[r];
+              nst += __popc(m);
+            }
+            if (nst > kStage - 128u) {  // room for the next four rounds
+              async_append(stb, nst, 0u);
+              nst = 0;
+            }
+          }
+          // one atomic reserves the staged claims' slots and counts this
+          // step's sources as expanded
+          async_append(stb, nst, (uint32_t)__popc(rmask));
+          pend = pend && !rdy;
+          continue;
+        }
+        // nothing filled: finished when every appended vertex is expanded.
+        // Checked on every eighth empty poll only: thousands of idle warps
+        // reading aq_td would queue ahead of the steps' atomics on it in its
+        // L2 slice.  Lane 0 decides for the warp, so the warp leaves as a
+        // whole.
+        uint32_t fin = 0;
+        if (lane == 0 && (++idle & 7u) == 0) {
+          const unsigned long long td = ld_acquire64(&c->aq_td);
+          fin = (uint32_t)(td >> 32) == (uint32_t)td || ldm(&c->gs.err) != 0;
+          if (!fin) {
+            const unsigned long long now = globaltimer_ns();
+            if (idle0 == 0) idle0 = now;
+            if (now - idle0 > P.o.timeout_ns) {
+              atomicOr(&c->gs.err, kErrBarrierTimeout);
+              atomicExch(&c->gs.err_where, 712u);
+              fin = 1;
+            }
+          }
+        }
+        if (__shfl_sync(kFull, fin, 0)) {
+          over = true;
+          break;
+        }
+        __nanosleep(nap);
+        if (nap < 256u) nap <<= 1;
+      }
+    }
+    add_count(cur() + C_CHG, lane == 0 ? steps : 0u);
+    if (!bar(711)) return;
+    if (is_lead()) c->phase_ret2 = rdprv(C_CHG);
+  }
+
   // Worklist reach: DATA / LINEAR / TOPO / BEST.  Levels are synchronous:
   // level k expands the vertices first reached in level k-1 (the pivots at
   // k = 0) and appends each vertex it reaches, exactly once, to the next
@@ -1340,7 +1625,7 @@ struct Eng {
   // than live / beta vertices are reached per sweep.
   __device__ uint32_t reach_wl(const uint32_t *__restrict__ off, const uint32_t *__restrict__ adj,
                                const uint32_t *__restrict__ poff, const uint32_t *__restrict__ padj, uint32_t *vis,
-                               bool ranged, bool balanced, bool allow_pull) {
+                               bool ranged, bool balanced, bool allow_pull, uint32_t async_from = kNone) {
     const EngState &s = P.s;
     const long long alpha = P.o.pull_alpha > 0 ? P.o.pull_alpha : 14;
     const long long beta = P.o.pull_beta > 0 ? P.o.pull_beta : 24;
@@ -1357,13 +1642,25 @@ struct Eng {
     // the last pull sweep tested list heads only: the next level must be a
     // full pull sweep over the remaining list, even with an empty frontier
     bool partial = false;
+    // thin, deep reaches continue asynchronously (the frontier's edges are
+    // known only where pulls are allowed)
+    const uint32_t async_after = async_from != kNone ? async_from : P.o.async_depth > 0 ? (uint32_t)P.o.async_depth : kNone;
     while (nin > 0 || partial) {
       const unsigned long long ts = globaltimer_ns();
+      if (allow_pull && !pull && !partial && depth >= async_after && mf <= (unsigned long long)nin * 8ull) {
+        async_reach(off, adj, vis, ranged, in, nin);
+        prof(PR_ASYNC, ts, (uint32_t)(ldm64(&c->aq_td) >> 32), ldm(&c->phase_ret2));  // vertices expanded, warp steps
+        ++depth;
+        break;
+      }
       // a small frontier goes to CTA 0; if it refuses (too many edges), the
       // grid expands this level as usual and the next level tries again
       if (!pull && !partial && nin <= kLocalMax) {
         const uint32_t room = P.o.max_iters > depth ? P.o.max_iters - depth : 0u;
-        if (blockIdx.x == 0) local_levels(off, adj, vis, ranged, in, nin, sel, room < kLocalLevels ? room : kLocalLevels);
+        uint32_t lroom = room < kLocalLevels ? room : kLocalLevels;
+        // a reach that may turn asynchronous stops its local levels there
+        if (allow_pull && depth < async_after && async_after - depth < lroom) lroom = async_after - depth;
+        if (blockIdx.x == 0) local_levels(off, adj, vis, ranged, in, nin, sel, lroom);
         if (!bar(704)) return depth;
         if (!rdprv(C_LREF) && rdprv(C_LD) > 0) {
           const uint32_t ld = rdprv(C_LD);
@@ -1428,7 +1725,8 @@ struct Eng {
         const unsigned long long per_warp = mf / nwarps();
         uint32_t split = heavy;
         if (allow_pull && per_warp < heavy) split = per_warp < 256ull ? 256u : (uint32_t)per_warp;
-        if (!push_level(off, adj, vis, ranged, allow_pull, in, nin, out, split, qoff)) return depth;
+        const bool wide = !allow_pull || mf <= (unsigned long long)nin * kWideDegree;
+        if (!push_level(off, adj, vis, ranged, allow_pull, in, nin, out, split, qoff, wide)) return depth;
       } else {
         rem_valid = false;
         data_level(off, adj, vis, ranged, in, nin, out);
@@ -1460,6 +1758,7 @@ struct Eng {
       case ARM_D: return reach_wl(off, adj, poff, padj, vis, ranged, false, false);
       case ARM_L: return reach_wl(off, adj, poff, padj, vis, ranged, true, false);
       case ARM_B: return reach_wl(off, adj, poff, padj, vis, ranged, true, true);
+      case ARM_TA: return reach_wl(off, adj, poff, padj, vis, ranged, true, true, 0u);
       default: return reach_wl(off, adj, poff, padj, vis, ranged, true, P.o.pull_alpha >= 0);
     }
   }
@@ -1551,29 +1850,74 @@ struct Eng {
     uint32_t it = 0;
     for (;;) {
       uint32_t chg = 0;
-      // called from divergent code (warp_gather tails, heavy chunks): no warp collectives
+      // called from divergent code (heavy chunks): no warp collectives
       auto relax = [&](uint32_t src, uint32_t u, uint32_t rsrc) {
         if (!live(s, u) || ldm(s.range + u) != rsrc) return;
         const uint32_t x = ldm(lab + u);
         if (x < ldm(lab + src)) chg += atomicMin(lab + src, x) > x;
       };
-      for_vertices([&](uint32_t v, bool valid) {
-        uint32_t b = 0, d = 0, rv = 0;
-        const bool lv = valid && live(s, v);
-        if (lv) {
-          rv = ldm(s.range + v);
-          b = ldg(g.off + v);
-          d = ldg(g.off + v + 1) - b;
-          if (d > heavy) {
-            heavy_push(s, v, b, d, rv);
-            d = 0;
+      // A sweep: every live vertex takes the smallest colour among its
+      // partition-mate out-neighbours, and jumps to its colour's colour.
+      // The next vertex's state, offsets and colour are loaded one
+      // iteration ahead; the warp's lists are walked 128 edges per round
+      // with each round's loads (list entry; bitmap word, partition and
+      // colour of the target) issued together.  Colours only decrease and
+      // every colour a vertex ever holds is one it reaches, so a stale
+      // colour read here costs at most a redundant atomicMin.
+      struct Pre {
+        uint32_t ew, rv, b, e, l;
+      };
+      auto load = [&](uint32_t v, bool valid) {
+        const uint32_t vv = valid ? v : 0u;
+        return Pre{ldm(s.elim + (vv >> 5)), ldm(s.range + vv), ldg(g.off + vv), ldg(g.off + vv + 1), ldm(lab + vv)};
+      };
+      for_vertices_pf(load, [&](uint32_t v, bool valid, const Pre &p) {
+        const bool lv = valid && !((p.ew >> (v & 31u)) & 1u);
+        uint32_t b = lv ? p.b : 0u, d = lv ? p.e - p.b : 0u;
+        if (d > heavy) {
+          heavy_push(s, v, b, d, p.rv);
+          d = 0;
+        }
+        // pointer jump, issued with the first round's loads
+        const uint32_t jl = lv ? ldm(lab + p.l) : kNone;
+        const uint32_t lane = lane_id();
+        const uint32_t incl = warp_incl_scan(d);
+        const uint32_t total = __shfl_sync(kFull, incl, 31);
+        const uint32_t excl = incl - d;
+        for (uint32_t e0 = 0; e0 < total; e0 += 128u) {
+          uint32_t u[4], src[4], rs[4], sl[4];
+          bool val[4];
+#pragma unroll
+          for (int r = 0; r < 4; ++r) {
+            const uint32_t e = e0 + 32u * r + lane;
+            uint32_t lo = 0;
+#pragma unroll
+            for (uint32_t sft = 16; sft >= 1; sft >>= 1) {
+              const uint32_t cand = lo + sft;
+              const uint32_t ex = __shfl_sync(kFull, excl, cand & 31u);
+              if (cand < 32 && ex <= e) lo = cand;
+            }
+            const uint32_t o_beg = __shfl_sync(kFull, b, lo), o_ex = __shfl_sync(kFull, excl, lo);
+            src[r] = __shfl_sync(kFull, v, lo);
+            rs[r] = __shfl_sync(kFull, p.rv, lo);
+            sl[r] = __shfl_sync(kFull, p.l, lo);
+            val[r] = e < total;
+            u[r] = val[r] ? ldg(g.adj + o_beg + (e - o_ex)) : 0u;
+          }
+          uint32_t ew[4], rg[4], lu[4];
+#pragma unroll
+          for (int r = 0; r < 4; ++r) {
+            ew[r] = val[r] ? ldm(s.elim + (u[r] >> 5)) : ~0u;
+            rg[r] = val[r] ? ldm(s.range + u[r]) : 0u;
+            lu[r] = val[r] ? ldm(lab + u[r]) : kNone;
+          }
+#pragma unroll
+          for (int r = 0; r < 4; ++r) {
+            const bool ok = val[r] && !((ew[r] >> (u[r] & 31u)) & 1u) && rg[r] == rs[r] && lu[r] < sl[r];
+            if (ok) chg += atomicMin(lab + src[r], lu[r]) > lu[r];
           }
         }
-        warp_gather(v, b, d, rv, g.adj, relax);
-        if (lv) {  // pointer jump
-          const uint32_t m = ldm(lab + v), j = ldm(lab + m);
-          if (j < m) chg += atomicMin(lab + v, j) > j;
-        }
+        if (lv && jl < p.l) chg += atomicMin(lab + v, jl) > jl;
       });
       add_count(cur() + C_CHG, chg);
       if (!bar(901)) return it;
@@ -1725,14 +2069,22 @@ struct Eng {
   }
 
   __device__ __forceinline__ uint32_t arm_for(bool below) const {
+    // graphs of more than kAsyncTailDegree edges per vertex keep QUADRATIC
+    // tails: theirs are few and short, and a sweep over the survivors costs
+    // less than an asynchronous reach's seeding and two barriers
+    const bool thin = (unsigned long long)P.g.m <= (unsigned long long)P.g.n * kAsyncTailDegree;
+    const uint32_t tail = P.o.async_depth < 0 || !thin ? ARM_Q : ARM_TA;
     switch (P.o.alg) {
       case 0: return ARM_Q;
       case 1: return ARM_T;
       case 2: return ARM_D;
       case 3: return ARM_L;
-      case 4: return below ? ARM_T : ARM_Q;  // HYBRID: reach_t below n/100, reach_q above
-      case 5: return below ? ARM_L : ARM_Q;  // COMBINE
-      case 6: return below ? ARM_B : ARM_Q;  // BEST
+      // past the switch point the reference sweeps (QUADRATIC); here the
+      // tails are asynchronous worklist reaches from all partitions' pivots
+      // at once unless async reaches are off (async_depth < 0)
+      case 4: return below ? ARM_T : tail;  // HYBRID: reach_t below n/100, reach_q above
+      case 5: return below ? ARM_L : tail;  // COMBINE
+      case 6: return below ? ARM_B : tail;  // BEST
       default: return ARM_T;
     }
   }
@@ -2063,7 +2415,12 @@ static cudaError_t coop_launch(const Params &p, uint32_t phase, uint32_t a0, uin
   if (e != cudaSuccess) return e;
   if (per_sm < 1) return cudaErrorInvalidConfiguration;
   uint32_t maxg = (uint32_t)(sms * per_sm);
-  uint32_t g = grid_blocks ? (grid_blocks < maxg ? grid_blocks : maxg) : maxg;
+  // default grid: every co-resident CTA, except for small graphs, which get
+  // one CTA per SM (their phases are barrier-bound, and a grid barrier
+  // costs less with fewer arrivals)
+  uint32_t g = maxg;
+  if (grid_blocks) g = grid_blocks < maxg ? grid_blocks : maxg;
+  else if (p.g.n <= kSmallGraphN && (uint32_t)sms < maxg) g = (uint32_t)sms;
   if (grid_used) *grid_used = g;
   Params pp = p;
   void *args[] = {&pp, &phase, &a0, &a1, &a2};

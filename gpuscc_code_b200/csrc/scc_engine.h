@@ -45,6 +45,10 @@ struct Ctl {
   uint32_t trace_n, trace_pad;
   uint32_t trace_slot[128], trace_a[128], trace_b[128];
   unsigned long long trace_ns[128];
+  // asynchronous reach: next slot to take; slots appended << 32 | vertices
+  // expanded (each in its own 128-byte line)
+  uint32_t aq_head, aq_pad0[31];
+  unsigned long long aq_td, aq_pad1[15];
 };
 constexpr uint32_t kTrace = 128;
 
@@ -62,6 +66,7 @@ enum Prof : uint32_t {
   PR_COMPACT = 10,
   PR_FINAL = 11,
   PR_PIVOT = 12,
+  PR_ASYNC = 13,     // asynchronous reach tails
   PR_COUNT = 16
 };
 
@@ -83,6 +88,7 @@ struct EngState {
   uint32_t *act[2];        // active lists, qcap each
   uint32_t *piv, *pivkey;  // pivot list, qcap each
   unsigned long long *slot;  // 3(n+1): partition-refinement pivot election, all ones between uses
+  uint32_t *aq;              // qcap: asynchronous reach queue, all ones (empty slots) between uses
   uint32_t *hv, *hbeg, *hdeg, *htag, *hbase;  // heavy adjacency list split across the grid
   const uint32_t *seg;       // nseg+1 segment first ids (device) or null
   uint32_t *out_labels;      // optional destination of the final labels (device)
@@ -101,7 +107,7 @@ struct EngOpts {
   uint32_t warp_degree, heavy_degree, max_iters;
   unsigned long long timeout_ns;
   int32_t trim_first_depth;
-  uint32_t pad;
+  int32_t async_depth;  // levels before a thin reach turns asynchronous; < 0: never
   unsigned long long test_stall_ns;  // fault-path test hook: last CTA stalls before barrier interval 1 ends
 };
 

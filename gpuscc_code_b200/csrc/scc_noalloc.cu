@@ -40,7 +40,7 @@ constexpr size_t a256(size_t x) { return (x + 255) & ~size_t(255); }
 constexpr uint32_t kWords = sccb::bitmap_words(kMaxN) + sccb::kBitmapSlack;
 constexpr size_t kVec = a256(size_t(kMaxN + 1) * 4);        // one u32 per vertex
 constexpr size_t kBitmaps = a256(size_t(kWords) * 4 * 7);   // elim, fvis, bvis, fexp, bexp, tflag, queued
-constexpr size_t kSlots = a256(size_t(kMaxN + 1) * 3 * 8);  // partition-election slots
+constexpr size_t kSlots = a256(size_t(kMaxN + 1) * (3 * 8 + 4));  // election slots + asynchronous reach queue
 constexpr uint32_t kHeavyCap = kMaxM / 256u + 2u;
 constexpr size_t kHeavy = a256(size_t(kHeavyCap) * 5 * 4);
 constexpr size_t kCtl = a256(sizeof(sccb::Ctl));
@@ -141,6 +141,7 @@ extern "C" int scc_solve_noalloc(const scc_dev_csr *g, const scc_opts *opts, uin
   s.tflag = bm + 5 * (size_t)kWords;
   s.queued = bm + 6 * (size_t)kWords;
   s.slot = reinterpret_cast<unsigned long long *>(cur);
+  s.aq = reinterpret_cast<uint32_t *>(s.slot + 3 * ((size_t)n + 1));
   cur += kSlots;
   uint32_t *h = reinterpret_cast<uint32_t *>(cur);
   cur += kHeavy;
@@ -173,13 +174,14 @@ extern "C" int scc_solve_noalloc(const scc_dev_csr *g, const scc_opts *opts, uin
   e.max_iters = o.max_iters ? o.max_iters : (1u << 20);
   e.timeout_ns = (unsigned long long)(o.timeout_ms ? o.timeout_ms : 10000u) * 1000000ull;
   e.trim_first_depth = o.trim_first_depth;
+  e.async_depth = o.async_depth ? o.async_depth : 4;
   e.test_stall_ns = (unsigned long long)o.test_stall_us * 1000ull;
   if (o.test_queue_cap && o.test_queue_cap < s.qcap) s.qcap = o.test_queue_cap;
   if (d_labels) s.label = d_labels;  // labels go straight to the caller's buffer
 
   // the array keeps the previous call's contents: reset what must start fresh
   cudaError_t err = cudaMemsetAsync(s.ctl, 0, sizeof(sccb::Ctl), st);
-  if (err == cudaSuccess) err = cudaMemsetAsync(s.slot, 0xff, ((size_t)n + 1) * 3 * 8, st);
+  if (err == cudaSuccess) err = cudaMemsetAsync(s.slot, 0xff, ((size_t)n + 1) * (3 * 8 + 4), st);
   if (err != cudaSuccess) return sccb::set_error(SCC_ERR_CUDA, "scratch reset: %s", cudaGetErrorString(err));
   for (int t = 0; t < 2; ++t) {
     uint32_t bad = 0;

@@ -187,6 +187,7 @@ class Options:
     timeout_ms: int = 0
     trim_first_depth: int = 1
     occupancy: int = 0
+    async_depth: int = 0
     test_stall_us: int = 0
     test_queue_cap: int = 0
 
@@ -335,7 +336,7 @@ class SCCContext:
         return int(cnt.value), st.as_dict()
 
     PROFILE_SLOTS = ["trim_sweep", "trim_worklist", "push", "pull", "heavy", "worklist_level", "quadratic",
-                     "update", "wcc", "trim2", "compact", "finalize", "first_pivot"]
+                     "update", "wcc", "trim2", "compact", "finalize", "first_pivot", "async"]
 
     def profile(self) -> dict:
         """Device-side phase timers of the last call: {slot: (ms, count)}."""

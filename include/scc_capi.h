@@ -79,12 +79,20 @@ typedef struct scc_opts {
   uint32_t warp_degree;    /* adjacency length from which a list is expanded by a whole warp (0 = 32) */
   uint32_t heavy_degree;   /* adjacency length from which a list is split across the grid (0 = 4096) */
   uint32_t max_iters;      /* cap on sweeps of any one fixpoint/reach loop and on FB rounds (0 = 1<<20) */
-  uint32_t grid_blocks;    /* persistent grid size (0 = every co-resident block) */
+  uint32_t grid_blocks;    /* persistent grid size (0 = every co-resident block; one block per SM for
+                              graphs of at most 2^21 vertices) */
   uint32_t timeout_ms;     /* bound on any device-side wait inside the persistent kernel (0 = 10000) */
   int32_t trim_first_depth;/* global trim-1 before the first pivot: 0 = to its fixpoint (reference trim1),
                               k > 0 = at most k iterations; later partition-aware trims remove the rest */
   int32_t occupancy;       /* register budget of the persistent kernel: 4 = four 256-thread CTAs per SM
                               (64 registers), 3 = three (80 registers); 0 = engine default (4) */
+  int32_t async_depth;     /* TOPO / BEST / HYBRID reaches: after this many synchronous levels, a frontier of
+                              at most 8 edges per vertex is expanded asynchronously (every warp takes queued
+                              vertices as they are appended, no level barriers; for deep, thin reaches such as
+                              grids), and on graphs of at most 12 edges per vertex the HYBRID / COMBINE /
+                              BEST tails past the switch point are asynchronous reaches instead of QUADRATIC
+                              sweeps; 0 = 4, -1 = never (the reference's synchronous levels and QUADRATIC
+                              tails).  Labels do not depend on it. */
   /* Fault-path test hooks (0 = off; labels are never affected while off).
    * test_stall_us: the last CTA of the grid waits this long (a bounded
    *   %globaltimer spin) before its second grid-barrier arrival, so that the

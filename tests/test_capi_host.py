@@ -39,9 +39,10 @@ def test_binding_covers_every_declared_symbol():
 
 
 def test_struct_sizes_match_the_header_layout():
-    assert C.sizeof(_capi.scc_opts) == 20 * 4
+    assert C.sizeof(_capi.scc_opts) == 21 * 4
     assert C.sizeof(_capi.scc_stats) == 16 * 4 + 6 * 8
-    assert C.sizeof(_capi.scc_server_cfg) == 6 * 4 + 8 + C.sizeof(_capi.scc_opts)
+    # the trailing scc_opts (4-byte aligned) is padded to the struct's 8-byte alignment
+    assert C.sizeof(_capi.scc_server_cfg) == (6 * 4 + 8 + C.sizeof(_capi.scc_opts) + 7) // 8 * 8
     assert C.sizeof(_capi.scc_request_info) == 6 * 4 + 3 * 8
 
 
