@@ -37,7 +37,10 @@ constexpr uint32_t kLocalMax = 2048, kLocalEdges = 4096, kLocalLevels = 4096;
 // targets with try_visit_wide
 constexpr uint32_t kWideDegree = 16;
 // polls of a partly filled window before an asynchronous step expands it
-constexpr uint32_t kAsyncHold = 2;
+constexpr uint32_t kAsyncHold = 1;
+// WCC switches from full sweeps to frontier sweeps once fewer than live / this
+// many colours change in a sweep
+constexpr uint32_t kWccFrontier = 64;
 // graphs of at most this many vertices run on one CTA per SM by default
 constexpr uint32_t kSmallGraphN = 1u << 21;
 // HYBRID / COMBINE / BEST tails are asynchronous reaches on graphs of at most
@@ -1503,7 +1506,7 @@ struct Eng {
         const uint32_t v = pend ? ldm(aq + slot) : kNone;
         const bool rdy = pend && v != kNone;
         const uint32_t rmask = __ballot_sync(kFull, rdy);
-        // a partly filled window is polled again once or twice before it is
+        // a partly filled window is polled once more before it is
         // expanded: while the reach is wide its other slots fill within
         // nanoseconds, and a step then expands up to 32 vertices, not two
         if (rmask && rmask != __ballot_sync(kFull, pend) && hold < kAsyncHold) {
@@ -1838,32 +1841,136 @@ struct Eng {
   // they label, so updates may land in any order (atomicMin) and the fixpoint
   // is the same.  Lists are walked warp-wide, lists longer than heavy_degree
   // by the whole grid.
+  // Appends the ids of every set bit of bm to out (counter cur()[C_Q]): a
+  // lane per bitmap word, one atomicAdd per warp-step.
+  __device__ __forceinline__ void bitmap_list(const uint32_t *bm, uint32_t *out) {
+    const EngState &s = P.s;
+    const uint32_t lane = lane_id();
+    for (uint32_t w0 = gwarp() * 32u; w0 < s.nwords; w0 += nwarps() * 32u) {
+      const uint32_t w = w0 + lane;
+      const uint32_t bits = w < s.nwords ? ldm(bm + w) : 0u;
+      const uint32_t cnt = __popc(bits);
+      const uint32_t incl = warp_incl_scan(cnt);
+      uint32_t base = 0;
+      if (lane == 31 && incl) base = atomicAdd(cur() + C_Q, incl);
+      base = __shfl_sync(kFull, base, 31);
+      uint32_t pos = base + incl - cnt;
+      for (uint32_t x = bits; x; x &= x - 1u) {
+        if (pos < s.qcap) out[pos] = w * 32u + (uint32_t)(__ffs(x) - 1);
+        else fail(kErrQueueOverflow);
+        ++pos;
+      }
+    }
+  }
+
+  // Frontier sweep of the WCC colouring: every vertex of cl[0, nc) (its
+  // colour fell in the last sweep; bit set in cbm) offers its colour to its
+  // live partition-mate in-neighbours; each one whose colour falls is
+  // claimed once in nbm and appended to out.  cbm's bits of cl are cleared
+  // on the way, so cbm is empty afterwards.
+  __device__ __noinline__ void wcc_push(const uint32_t *cl, uint32_t nc, uint32_t *cbm, uint32_t *nbm, uint32_t *out) {
+    const EngState &s = P.s;
+    const EngGraph &g = P.g;
+    uint32_t *lab = s.aux;
+    Stage oq = stage_open(0, out, cur() + C_Q, s.qcap);
+    for_items(nc, [&](uint32_t i, bool valid) {
+      uint32_t v = 0, b = 0, d = 0, rv = 0, lv = kNone;
+      if (valid) {
+        v = ldm(cl + i);
+        bit_clear(cbm, v);
+        b = ldg(g.offT + v);
+        d = ldg(g.offT + v + 1) - b;
+        rv = ldm(s.range + v);
+        lv = ldm(lab + v);
+      }
+      warp_gather_all(lv, b, d, rv, g.adjT, [&](uint32_t l, uint32_t w, uint32_t rsrc, bool ok) {
+        bool claimed = false;
+        if (ok) {
+          const uint32_t ww = w >> 5, bit = 1u << (w & 31u);
+          const uint32_t ew = ldm(s.elim + ww), rw = ldm(s.range + w), lw = ldm(lab + w);
+          if (!(ew & bit) && rw == rsrc && l < lw && atomicMin(lab + w, l) > l) claimed = bit_claim(nbm, w);
+        }
+        stage_put(oq, claimed, w);
+      });
+    });
+    stage_flush(oq);
+  }
+
+  // ============================================================ WCC (a15)
+  // wcc.cu:7-144: colour of a live vertex = the smallest id it reaches
+  // through out-edges between live partition-mates.  Full sweeps (every
+  // live vertex takes its out-neighbours' smallest colour and jumps to its
+  // colour's colour) while many colours change; they record the vertices
+  // whose colour fell in a bitmap (fexp / bexp alternately: both are empty
+  // from unset_pivots until the next reach).  Once fewer than live/64
+  // colours changed in a sweep, those vertices form a list and later sweeps
+  // push colours from the changed vertices to their in-neighbours only
+  // (wcc_push): the tail of long, thin chains then costs a few items per
+  // sweep instead of a sweep over every live vertex.  Both modes reach the
+  // same fixpoint: after a full sweep, only a vertex whose colour fell
+  // during it can still lower an in-neighbour's colour, and every such
+  // vertex is in the list.
   __device__ __noinline__ uint32_t wcc() {
     const EngState &s = P.s;
     const EngGraph &g = P.g;
     const uint32_t heavy = P.o.heavy_degree;
     uint32_t *lab = s.aux;
+    uint32_t *const bm[2] = {s.fexp, s.bexp};
+    for (uint32_t w = gtid(); w < s.nwords; w += gstride()) {
+      s.fexp[w] = 0u;
+      s.bexp[w] = 0u;
+    }
     for_vertices([&](uint32_t v, bool valid) {
       if (valid && live(s, v)) lab[v] = v;
     });
     if (!bar(900)) return 0;
+    const uint32_t nlive = ldm(&c->n_live);
     uint32_t it = 0;
+    bool front = false;
+    uint32_t nc = 0, cb = 0;  // frontier length, bitmap holding its members
+    uint32_t *cl = s.qa, *cn = s.qb;
     for (;;) {
+      const unsigned long long tw = globaltimer_ns();
+      if (front) {
+        wcc_push(cl, nc, bm[cb], bm[cb ^ 1u], cn);
+        if (!bar(905)) return it;
+        nc = rdprv(C_Q);
+        uint32_t *t = cl;
+        cl = cn;
+        cn = t;
+        cb ^= 1u;
+        ++it;
+        prof(PR_WCC_IT, tw, nc, 1u);
+        if (nc == 0) break;
+        if (it >= P.o.max_iters) {
+          fail(kErrIterCap);
+          break;
+        }
+        continue;
+      }
       uint32_t chg = 0;
+      uint32_t *const mk = bm[it & 1u];
+      // the other bitmap (marks of the sweep before) is cleared for the next
+      for (uint32_t w = gtid(); w < s.nwords; w += gstride()) bm[(it + 1u) & 1u][w] = 0u;
+      auto lower = [&](uint32_t v, uint32_t x) {
+        if (atomicMin(lab + v, x) > x) {
+          ++chg;
+          bit_set(mk, v);
+        }
+      };
       // called from divergent code (heavy chunks): no warp collectives
       auto relax = [&](uint32_t src, uint32_t u, uint32_t rsrc) {
         if (!live(s, u) || ldm(s.range + u) != rsrc) return;
         const uint32_t x = ldm(lab + u);
-        if (x < ldm(lab + src)) chg += atomicMin(lab + src, x) > x;
+        if (x < ldm(lab + src)) lower(src, x);
       };
-      // A sweep: every live vertex takes the smallest colour among its
-      // partition-mate out-neighbours, and jumps to its colour's colour.
       // The next vertex's state, offsets and colour are loaded one
       // iteration ahead; the warp's lists are walked 128 edges per round
       // with each round's loads (list entry; bitmap word, partition and
       // colour of the target) issued together.  Colours only decrease and
       // every colour a vertex ever holds is one it reaches, so a stale
-      // colour read here costs at most a redundant atomicMin.
+      // colour read here costs at most a redundant atomicMin (and a sweep
+      // with no change read only current colours).
       struct Pre {
         uint32_t ew, rv, b, e, l;
       };
@@ -1914,10 +2021,10 @@ struct Eng {
 #pragma unroll
           for (int r = 0; r < 4; ++r) {
             const bool ok = val[r] && !((ew[r] >> (u[r] & 31u)) & 1u) && rg[r] == rs[r] && lu[r] < sl[r];
-            if (ok) chg += atomicMin(lab + src[r], lu[r]) > lu[r];
+            if (ok) lower(src[r], lu[r]);
           }
         }
-        if (lv && jl < p.l) chg += atomicMin(lab + v, jl) > jl;
+        if (lv && jl < p.l) lower(v, jl);
       });
       add_count(cur() + C_CHG, chg);
       if (!bar(901)) return it;
@@ -1930,10 +2037,20 @@ struct Eng {
         if (!bar(904)) return it;
       }
       ++it;
-      if (rdprv(C_CHG) == 0) break;
+      const uint32_t nchg = rdprv(C_CHG);
+      prof(PR_WCC_IT, tw, nchg, list_mode ? act_count : P.g.n);
+      if (nchg == 0) break;
       if (it >= P.o.max_iters) {
         fail(kErrIterCap);
         break;
+      }
+      if ((unsigned long long)nchg * kWccFrontier < nlive) {
+        // the marked vertices become the frontier list (mk = bm[(it - 1) & 1])
+        bitmap_list(mk, cl);
+        if (!bar(906)) return it;
+        nc = rdprv(C_Q);
+        cb = (it - 1u) & 1u;
+        front = true;
       }
     }
     // roots become pivots of fresh partitions; members join their root's

@@ -67,6 +67,7 @@ enum Prof : uint32_t {
   PR_FINAL = 11,
   PR_PIVOT = 12,
   PR_ASYNC = 13,     // asynchronous reach tails
+  PR_WCC_IT = 14,    // one WCC relaxation sweep
   PR_COUNT = 16
 };
 

@@ -336,7 +336,7 @@ class SCCContext:
         return int(cnt.value), st.as_dict()
 
     PROFILE_SLOTS = ["trim_sweep", "trim_worklist", "push", "pull", "heavy", "worklist_level", "quadratic",
-                     "update", "wcc", "trim2", "compact", "finalize", "first_pivot", "async"]
+                     "update", "wcc", "trim2", "compact", "finalize", "first_pivot", "async", "wcc_sweep"]
 
     def profile(self) -> dict:
         """Device-side phase timers of the last call: {slot: (ms, count)}."""
