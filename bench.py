@@ -374,7 +374,8 @@ def run_ours(args) -> None:
     workloads = None
     if world == 1 and not args.no_workloads:
         workloads = {}
-        for name, fn in (("grid", measure_grid), ("batch", measure_batch), ("serve", measure_serve)):
+        for name, fn in (("small", measure_small), ("grid", measure_grid), ("batch", measure_batch),
+                         ("serve", measure_serve)):
             t0 = time.perf_counter()
             try:
                 workloads[name] = fn(args)
@@ -438,6 +439,89 @@ def _events_ms(stream, fn, steps: int):
     return out
 
 
+def _ref_gpu_leg(cli: list, count: int, ours_ms: float, timeout: int) -> dict:
+    """The reference's own GPU FB (scc_2_w build, -a h) on the same graph in a
+    child process: its own timer, against this engine's device time."""
+    import subprocess
+
+    from oracle import ref_gpu
+
+    if not ref_gpu.available():
+        return {"unavailable": "oracle/_ref/libscc_ref_gpu.so not built"}
+    try:
+        r = subprocess.run([sys.executable, "-m", "oracle.ref_gpu", *cli, "--alg", "h"], cwd=ROOT,
+                           capture_output=True, text=True, timeout=timeout)
+        ref = json.loads(r.stdout.strip().splitlines()[-1]) if r.returncode == 0 else {
+            "error": f"exit {r.returncode}: {(r.stderr or r.stdout).strip()[-200:]}"}
+    except subprocess.TimeoutExpired:
+        ref = {"error": f"no result within {timeout} s"}
+    if "secs" in ref:
+        ref["count_matches"] = ref["nscc"] == count
+        ref["speedup_of_ours"] = ref["secs"] * 1e3 / ours_ms
+    return ref
+
+
+def measure_small(args) -> dict:
+    """R-MAT 2^16 vertices, 2^20 samples, seed 1 (config 1): the small-graph
+    latency of one solve (scc_2_w -a h) on the device, end to end through
+    scc_solve from pinned buffers, the reference's Tarjan on one host thread,
+    the reference's GPU FB on the same graph, parity."""
+    import torch
+
+    import gpuscc_code_b200 as scc
+
+    gh = scc.gen_rmat(16, 1 << 20, seed=1)
+    n, m = gh.n, gh.m
+    ctx = scc.SCCContext(0, scc.Options(alg="h", wcc=True, trim2=True))
+    ctx.upload(gh)
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    for _ in range(5):
+        cnt, st = ctx.solve_device()
+    sampler = ClockSampler(0).start()
+    ms = _events_ms(stream, lambda: ctx.solve_enqueue(), max(50, args.workload_steps))
+    cnt, st = ctx.solve_collect()
+    clocks = sampler.stop().summary()
+    prof = ctx.profile()
+    dev_ms = statistics.median(ms)
+    arrs = [pinned_u32(n + 2), pinned_u32(m), pinned_u32(n + 2), pinned_u32(m)]
+    for a, src in zip(arrs, (gh.nodes, gh.edges, gh.nodesT, gh.edgesT)):
+        a[:len(src)] = src
+    hp = scc.HostCSR.from_arrays(arrs[0], arrs[1][:m], arrs[2], arrs[3][:m], sorted_unique=True)
+    out = pinned_u32(n + 1)
+    for _ in range(3):
+        ctx.upload(hp)
+        ctx.solve(out=out)
+    reps = 20
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        ctx.upload(hp)
+        _, c2, st2 = ctx.solve(out=out)
+    e2e_s = (time.perf_counter() - t0) / reps
+    ctx.close()
+    peak, peak_kind = load_peaks()
+    achieved = b_alg(n, m) / (dev_ms / 1e3) / 1e9
+    secs, rcnt, kind = cpu_tarjan(n, gh.nodes, gh.edges)
+    return {
+        "metric": "SCC solve latency (R-MAT 2^16, 2^20 samples, seed 1, scc_2_w -a h)",
+        "value": dev_ms, "unit": "ms", "higher_is_better": False, "edges_per_s": m / (dev_ms / 1e3),
+        "steps": len(ms), "ms_all": [round(x, 4) for x in ms],
+        "config": {"workload": "rmat16_e20_seed1_scc_2_w", "n": n, "m": m, "nscc": cnt, "rounds": st.get("steps"),
+                   "grid_blocks": st.get("grid_blocks"), "l2": "graph fits in L2 (8.5 MB); no flush: the "
+                   "latency of back-to-back solves of a resident graph"},
+        "roofline": {"bound": "latency", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_kind": peak_kind, "algorithmic_bytes": b_alg(n, m)},
+        "e2e": {"value": e2e_s * 1e3, "unit": "ms", "h2d_bytes_per_step": 8 * (n + 2) + 8 * m,
+                "d2h_bytes_per_step": 4 * (n + 1)},
+        "cpu_baseline": {"value": secs * 1e3, "unit": "ms", "cores": 1, "kind": kind, "count": rcnt,
+                         "sample": "the whole graph, one Tarjan on 1 host thread"},
+        "reference_gpu_fb": _ref_gpu_leg(["--rmat", "16", "--samples-log2", "20", "--seed", "1"], cnt, dev_ms,
+                                         args.refgpu_timeout),
+        "parity": tarjan_parity("R-MAT 2^16, 2^20 samples, seed 1", n, gh.nodes, gh.edges, out, c2,
+                                st2.get("largest_scc")),
+        "clocks": clocks, "profile_ms": prof, "gpu_launches": 2 * len(ms),
+    }
+
+
 def measure_grid(args) -> dict:
     """4096^2 grid (config 3): every grid edge oriented by a coin flip, 15 %
     kept in both directions, long-range edges numbering 0.1 % of the grid
@@ -491,6 +575,7 @@ def measure_grid(args) -> dict:
                 "h2d_bytes_per_step": 8 * (n + 2) + 8 * m, "d2h_bytes_per_step": 4 * (n + 1)},
         "cpu_baseline": {"value": m / secs, "unit": UNIT, "cores": 1, "kind": kind, "count": rcnt,
                          "sample": "the whole grid graph, one Tarjan on 1 host thread"},
+        "reference_gpu_fb": _ref_gpu_leg(["--grid", str(side), "--seed", "3"], cnt, dev_ms, args.refgpu_timeout),
         "parity": tarjan_parity(f"grid {side}^2, seed 3", n, gh.nodes, gh.edges, out, c2, st2.get("largest_scc")),
         "clocks": clocks, "profile_ms": prof, "gpu_launches": 2 * len(ms),
     }
@@ -724,7 +809,7 @@ def run_workload(args) -> None:
     import torch
 
     torch.cuda.set_device(0)
-    fn = {"grid": measure_grid, "batch": measure_batch, "serve": measure_serve}[args.workload]
+    fn = {"small": measure_small, "grid": measure_grid, "batch": measure_batch, "serve": measure_serve}[args.workload]
     res = fn(args)
     res.setdefault("n_gpus", 1)
     print(json.dumps(res), flush=True)
@@ -860,7 +945,7 @@ def main():
     ap.add_argument("--refgpu-algs", nargs="*", default=["h", "t"], help="refgpu: reference -a arms")
     ap.add_argument("--refgpu-timeout", type=int, default=300)
     ap.add_argument("--refgpu-batch", type=int, default=256, help="batch: graphs the reference GPU FB solves")
-    ap.add_argument("--workload", choices=["rmat26", "grid", "batch", "serve", "refgpu"], default="rmat26",
+    ap.add_argument("--workload", choices=["rmat26", "small", "grid", "batch", "serve", "refgpu"], default="rmat26",
                     help="rmat26: the headline line (with the other workloads inside it); grid / batch / serve: "
                          "one workload alone; refgpu: the reference's GPU FB on the same graphs")
     ap.add_argument("--serve-pool", type=int, default=24, help="serve: distinct graphs in the stream")

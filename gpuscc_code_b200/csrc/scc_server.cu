@@ -549,6 +549,9 @@ int scc_server::run_batch(std::vector<Request *> &batch) {
   return SCC_OK;
 }
 
+// at most four edges per vertex: the deep, thin graphs (grids) of a stream
+static bool is_thin(uint32_t n, uint32_t m) { return (uint64_t)m <= 4ull * n; }
+
 void scc_server::solve_loop() {
   cudaSetDevice(cfg.device);
   const uint32_t max_g = cfg.batching ? (cfg.max_batch_graphs ? cfg.max_batch_graphs : 256) : 1;
@@ -580,6 +583,9 @@ void scc_server::solve_loop() {
         if (!batch.empty() && batch[0]->g().n > cfg.solo_vertices) break;  // a large graph goes alone
         if (!batch.empty() && gn > cfg.solo_vertices) continue;
         if (!batch.empty() && std::memcmp(r->choice, batch[0]->choice, sizeof(r->choice)) != 0) continue;
+        // a batch runs as many rounds and levels as its deepest graph: thin
+        // graphs (grids: thousands of levels) are batched only with each other
+        if (!batch.empty() && is_thin(r->g().n, gm) != is_thin(batch[0]->g().n, batch[0]->g().m)) continue;
         if (!batch.empty() && (nv + gn > cfg.max_batch_vertices || ne + gm > cfg.max_batch_edges)) continue;
         batch.push_back(r);
         nv += gn;

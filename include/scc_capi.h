@@ -393,7 +393,9 @@ int scc_mlp_apply(const int32_t *choice, scc_opts *opts);
  * device frees up (one segmented persistent launch per batch; a graph alone
  * is bound in place).
  * With a strategy network loaded, each request's options come from it and
- * only requests with the same options share a batch. */
+ * only requests with the same options share a batch.  A batch runs as many
+ * rounds and levels as its deepest graph, so thin graphs (at most four edges
+ * per vertex, e.g. grids) share batches only with other thin graphs. */
 typedef struct scc_server scc_server;
 typedef struct scc_server_cfg {
   int32_t device;
