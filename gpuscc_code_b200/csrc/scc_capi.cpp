@@ -149,8 +149,9 @@ int ensure_state(scc_ctx *c) {
   CK(c->act1.ensure(vb), "alloc active list");
   CK(c->piv.ensure(vb), "alloc pivot list");
   CK(c->pivkey.ensure(vb), "alloc pivot keys");
-  // election slots, then the asynchronous reach queue: both all ones between uses
-  const size_t slot_bytes = ((size_t)cn + 1) * 3 * 8 + ((size_t)cn + 1) * 4;
+  // election slots, then the asynchronous reach queue (2(n+1) entries: both
+  // directions): both all ones between uses
+  const size_t slot_bytes = ((size_t)cn + 1) * 3 * 8 + ((size_t)cn + 1) * 8;
   if (slot_bytes > c->slot.bytes) c->slot_dirty = true;
   CK(c->slot.ensure(slot_bytes), "alloc election slots");
   CK(c->heavy.ensure((size_t)ch * 5 * 4), "alloc heavy list");
@@ -286,11 +287,14 @@ int verify_segments(scc_ctx *c) {
   return SCC_OK;
 }
 
+// fresh_ctl: the control block (barrier arrivals included) was just cleared
+// by the init kernel, so no separate clear is enqueued
 int launch(scc_ctx *c, uint32_t phase, uint32_t a0 = 0, uint32_t a1 = 0, uint32_t a2 = 0,
-           uint32_t *out_labels = nullptr) {
+           uint32_t *out_labels = nullptr, bool fresh_ctl = false) {
   const sccb::Params p = make_params(c, out_labels);
   // the grid barrier counts arrivals from zero in every launch
-  CK(cudaMemsetAsync(&p.s.ctl->gs.arrived, 0, sizeof(p.s.ctl->gs.arrived), c->stream), "clear barrier");
+  if (!fresh_ctl)
+    CK(cudaMemsetAsync(&p.s.ctl->gs.arrived, 0, sizeof(p.s.ctl->gs.arrived), c->stream), "clear barrier");
   CK(sccb::launch_phase(p, phase, a0, a1, a2, block_size_of(c), c->opts.grid_blocks, c->stream, &c->grid_used,
                         c->opts.occupancy),
      "cooperative launch");
@@ -302,8 +306,7 @@ int reset_state(scc_ctx *c) {
   int rc = ensure_state(c);
   if (rc) return rc;
   CK(cudaGetLastError(), "pending CUDA error before the solve");
-  CK(cudaMemsetAsync(c->ctl.p, 0, sizeof(sccb::Ctl), c->stream), "clear control block");
-  CK(cudaGetLastError(), "clear control block (deferred)");
+  // the init kernel also clears the control block
   const sccb::Params p = make_params(c, nullptr);
   CK(sccb::launch_init(p, c->stream), "init launch");
   ++c->launches;
@@ -707,7 +710,7 @@ int scc_solve_enqueue(scc_ctx *c, uint32_t *d_labels) {
   CK(cudaStreamIsCapturing(c->stream, &cs), "capture status");
   const bool timed = cs == cudaStreamCaptureStatusNone;
   if (timed) CK(cudaEventRecord(c->ev0, c->stream), "event");
-  rc = launch(c, sccb::PH_SOLVE, 0, 0, 0, d_labels);
+  rc = launch(c, sccb::PH_SOLVE, 0, 0, 0, d_labels, true);
   if (rc) return rc;
   if (timed) CK(cudaEventRecord(c->ev1, c->stream), "event");
   c->enq_labels = d_labels;

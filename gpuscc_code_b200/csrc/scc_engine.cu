@@ -57,8 +57,13 @@ struct Eng {
   Ctl *c;
   uint32_t k;  // barrier interval index, identical in every CTA
   uint32_t list_mode, act_count, act_sel;
+  // asynchronous reach: items seeded for the pending phase; a_defer: a
+  // reach seeds and returns, and the caller runs both directions' phase
+  uint32_t a_seeded;
+  bool a_defer;
 
-  __device__ explicit Eng(const Params &p) : P(p), c(p.s.ctl), k(0), list_mode(0), act_count(0), act_sel(0) {}
+  __device__ explicit Eng(const Params &p)
+      : P(p), c(p.s.ctl), k(0), list_mode(0), act_count(0), act_sel(0), a_seeded(0), a_defer(false) {}
 
   // ------------------------------------------------------------ plumbing
   __device__ __forceinline__ uint32_t *cur() { return c->ctr[k % 3]; }
@@ -1443,11 +1448,14 @@ struct Eng {
     }
   }
 
-  // Asynchronous tail of a worklist reach (no levels).  A deep, thin reach
+  // Asynchronous tail of worklist reaches (no levels).  A deep, thin reach
   // (a grid's thousands of levels of a few thousand vertices) is bound by
   // per-level latency -- a grid barrier plus the dependent loads of one
   // expansion -- not by bytes.  Reachability does not need levels: the
-  // frontier in[0, nin) is copied into the queue aq, and from then on every
+  // frontier is copied into the queue aq (async_seed; in the solve the
+  // forward and the backward reach both seed it, items tagged with their
+  // direction in bit 31, and their asynchronous parts run as one phase, so
+  // a round costs the deeper of the two reaches, not their sum); every
   // warp repeatedly takes the next 32 slots (one atomicAdd on aq_head),
   // expands the vertices of its slots as they are filled (the 32 lists
   // walked as one concatenation, 128 edges per round of loads), and appends
@@ -1468,25 +1476,33 @@ struct Eng {
     if (lane_id() == 0 && (k | done)) old = atomicAdd(&c->aq_td, ((unsigned long long)k << 32) | done);
     const uint32_t pos = (uint32_t)(__shfl_sync(kFull, old, 0) >> 32);
     for (uint32_t i = lane_id(); i < k; i += 32u) {
-      if (pos + i < P.s.qcap) P.s.aq[pos + i] = stb[i];
+      if (pos + i < 2u * P.s.qcap) P.s.aq[pos + i] = stb[i];
       else fail(kErrQueueOverflow);
     }
     __syncwarp();
   }
 
-  __device__ __noinline__ void async_reach(const uint32_t *__restrict__ off, const uint32_t *__restrict__ adj,
-                                           uint32_t *vis, bool ranged, const uint32_t *in, uint32_t nin) {
-    const EngState &s = P.s;
-    uint32_t *aq = s.aq;
-    const uint32_t qcap = s.qcap;
-    const uint32_t nseed = nin < qcap ? nin : qcap;
-    for_items(nseed, [&](uint32_t i, bool valid) {
-      if (valid) aq[i] = ldm(in + i);
+  // Appends the frontier in[0, nin) of direction dir to the asynchronous
+  // queue at slot `at` (every CTA calls it with the same arguments; the
+  // items are read after a later grid barrier).
+  __device__ __forceinline__ void async_seed(const uint32_t *in, uint32_t nin, uint32_t at, uint32_t dir) {
+    const uint32_t cap = 2u * P.s.qcap;
+    for_items(nin, [&](uint32_t i, bool valid) {
+      if (valid && at + i < cap) P.s.aq[at + i] = ldm(in + i) | (dir << 31);
     });
+    if (is_lead() && at + nin > cap) fail(kErrQueueOverflow);
+  }
+
+  // Expands the ntot items seeded in aq (bit 31: 0 = forward, 1 =
+  // backward) and everything they reach, both directions at once.
+  __device__ __noinline__ void async_run(uint32_t ntot, bool ranged) {
+    const EngState &s = P.s;
+    const EngGraph &g = P.g;
+    uint32_t *aq = s.aq;
+    const uint32_t qcap = 2u * s.qcap;
     if (is_lead()) {
-      if (nin > qcap) fail(kErrQueueOverflow);
       c->aq_head = 0;
-      c->aq_td = (unsigned long long)nin << 32;
+      c->aq_td = (unsigned long long)ntot << 32;
     }
     if (!bar(710)) return;
     const uint32_t lane = lane_id();
@@ -1521,10 +1537,12 @@ struct Eng {
           hold = 0;
           ++steps;
           uint32_t b = 0, d = 0, rv = 0;
+          const uint32_t dir = rdy ? v >> 31 : 0u, x = v & 0x7fffffffu;
           if (rdy) {
-            b = ldg(off + v);
-            d = ldg(off + v + 1) - b;
-            rv = ranged ? ldm(s.range + v) : 0u;
+            const uint32_t *off = dir ? g.offT : g.off;
+            b = ldg(off + x);
+            d = ldg(off + x + 1) - b;
+            rv = ranged ? ldm(s.range + x) : 0u;
             aq[slot] = kNone;
           }
           // the 32 lists walked as one concatenation, four 32-edge rounds
@@ -1535,7 +1553,7 @@ struct Eng {
           const uint32_t excl = incl - d;
           uint32_t nst = 0;  // staged claims (warp-uniform)
           for (uint32_t e0 = 0; e0 < total; e0 += 128u) {
-            uint32_t u[4], rs[4];
+            uint32_t u[4], rs[4], dr[4];
             bool val[4];
 #pragma unroll
             for (int r = 0; r < 4; ++r) {
@@ -1549,13 +1567,14 @@ struct Eng {
               }
               const uint32_t o_beg = __shfl_sync(kFull, b, lo), o_ex = __shfl_sync(kFull, excl, lo);
               rs[r] = __shfl_sync(kFull, rv, lo);
+              dr[r] = __shfl_sync(kFull, dir, lo);
               val[r] = e < total;
-              u[r] = val[r] ? ldg(adj + o_beg + (e - o_ex)) : 0u;
+              u[r] = val[r] ? ldg((dr[r] ? g.adjT : g.adj) + o_beg + (e - o_ex)) : 0u;
             }
             uint32_t vw[4], ew[4], rg[4];
 #pragma unroll
             for (int r = 0; r < 4; ++r) {
-              vw[r] = val[r] ? ldm(vis + (u[r] >> 5)) : ~0u;
+              vw[r] = val[r] ? ldm((dr[r] ? s.bvis : s.fvis) + (u[r] >> 5)) : ~0u;
               ew[r] = val[r] ? ldm(s.elim + (u[r] >> 5)) : ~0u;
               rg[r] = val[r] && ranged ? ldm(s.range + u[r]) : rs[r];
             }
@@ -1563,12 +1582,13 @@ struct Eng {
 #pragma unroll
             for (int r = 0; r < 4; ++r) {
               const uint32_t bit = 1u << (u[r] & 31u);
-              cl[r] = !((vw[r] | ew[r]) & bit) && rg[r] == rs[r] && !(atomicOr(vis + (u[r] >> 5), bit) & bit);
+              cl[r] = !((vw[r] | ew[r]) & bit) && rg[r] == rs[r] &&
+                      !(atomicOr((dr[r] ? s.bvis : s.fvis) + (u[r] >> 5), bit) & bit);
             }
 #pragma unroll
             for (int r = 0; r < 4; ++r) {
               const uint32_t m = __ballot_sync(kFull, cl[r]);
-              if (cl[r]) stb[nst + __popc(m & lanemask_lt())] = u[r];
+              if (cl[r]) stb[nst + __popc(m & lanemask_lt())] = u[r] | (dr[r] << 31);
               nst += __popc(m);
             }
             if (nst > kStage - 128u) {  // room for the next four rounds
@@ -1628,7 +1648,7 @@ struct Eng {
   // than live / beta vertices are reached per sweep.
   __device__ uint32_t reach_wl(const uint32_t *__restrict__ off, const uint32_t *__restrict__ adj,
                                const uint32_t *__restrict__ poff, const uint32_t *__restrict__ padj, uint32_t *vis,
-                               bool ranged, bool balanced, bool allow_pull, uint32_t async_from = kNone) {
+                               bool ranged, bool balanced, bool allow_pull, uint32_t dir, uint32_t async_from = kNone) {
     const EngState &s = P.s;
     const long long alpha = P.o.pull_alpha > 0 ? P.o.pull_alpha : 14;
     const long long beta = P.o.pull_beta > 0 ? P.o.pull_beta : 24;
@@ -1651,9 +1671,12 @@ struct Eng {
     while (nin > 0 || partial) {
       const unsigned long long ts = globaltimer_ns();
       if (allow_pull && !pull && !partial && depth >= async_after && mf <= (unsigned long long)nin * 8ull) {
-        async_reach(off, adj, vis, ranged, in, nin);
-        prof(PR_ASYNC, ts, (uint32_t)(ldm64(&c->aq_td) >> 32), ldm(&c->phase_ret2));  // vertices expanded, warp steps
+        // the frontier goes to the asynchronous queue; with a_defer the
+        // other direction's reach runs first and both finish together
+        async_seed(in, nin, a_seeded, dir);
+        a_seeded += nin;
         ++depth;
+        if (!a_defer) async_finish(ranged);
         break;
       }
       // a small frontier goes to CTA 0; if it refuses (too many edges), the
@@ -1750,6 +1773,15 @@ struct Eng {
     return depth;
   }
 
+  // Runs the asynchronous phase for whatever reaches seeded it.
+  __device__ void async_finish(bool ranged) {
+    if (a_seeded == 0) return;
+    const unsigned long long ts = globaltimer_ns();
+    async_run(a_seeded, ranged);
+    prof(PR_ASYNC, ts, (uint32_t)(ldm64(&c->aq_td) >> 32), ldm(&c->phase_ret2));  // vertices expanded, warp steps
+    a_seeded = 0;
+  }
+
   __device__ uint32_t reach(uint32_t dir, uint32_t arm, bool ranged) {
     const EngGraph &g = P.g;
     const EngState &s = P.s;
@@ -1758,11 +1790,11 @@ struct Eng {
     uint32_t *vis = dir ? s.bvis : s.fvis, *exp = dir ? s.bexp : s.fexp;
     switch (arm) {
       case ARM_Q: return reach_q(off, adj, vis, exp, ranged);
-      case ARM_D: return reach_wl(off, adj, poff, padj, vis, ranged, false, false);
-      case ARM_L: return reach_wl(off, adj, poff, padj, vis, ranged, true, false);
-      case ARM_B: return reach_wl(off, adj, poff, padj, vis, ranged, true, true);
-      case ARM_TA: return reach_wl(off, adj, poff, padj, vis, ranged, true, true, 0u);
-      default: return reach_wl(off, adj, poff, padj, vis, ranged, true, P.o.pull_alpha >= 0);
+      case ARM_D: return reach_wl(off, adj, poff, padj, vis, ranged, false, false, dir);
+      case ARM_L: return reach_wl(off, adj, poff, padj, vis, ranged, true, false, dir);
+      case ARM_B: return reach_wl(off, adj, poff, padj, vis, ranged, true, true, dir);
+      case ARM_TA: return reach_wl(off, adj, poff, padj, vis, ranged, true, true, dir, 0u);
+      default: return reach_wl(off, adj, poff, padj, vis, ranged, true, P.o.pull_alpha >= 0, dir);
     }
   }
 
@@ -2261,11 +2293,16 @@ struct Eng {
       // batch, or the graph) and no edge leaves a segment, so the reach and
       // trim of that round need no partition test.
       const bool ranged = step != 1;
+      // reaches that turn asynchronous leave their frontiers in the queue,
+      // and the two directions' asynchronous parts run as one phase
+      a_defer = true;
       t0 = globaltimer_ns();
       const uint32_t fd = reach(0, arm, ranged);
       timed(c->ns_fwd, t0);
       t0 = globaltimer_ns();
       const uint32_t bd = reach(1, arm, ranged);
+      a_defer = false;
+      async_finish(ranged);
       timed(c->ns_bwd, t0);
       t0 = globaltimer_ns();
       uint32_t ti = 0;
@@ -2395,6 +2432,11 @@ __global__ void __launch_bounds__(BS, MINB) scc_persistent(const __grid_constant
 __global__ void scc_init_kernel(Params p) {
   const uint32_t n = p.g.n;
   const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
+  if (blockIdx.x == 0) {  // the control block starts at zero (barrier arrivals included)
+    uint32_t *w = reinterpret_cast<uint32_t *>(p.s.ctl);
+    for (uint32_t i = threadIdx.x; i < sizeof(Ctl) / 4; i += blockDim.x) w[i] = 0u;
+    __syncthreads();
+  }
   for (uint32_t v = tid; v <= n; v += stride) {
     uint32_t r = 0;
     if (p.s.nseg > 1 && v >= 1) {

@@ -89,7 +89,7 @@ struct EngState {
   uint32_t *act[2];        // active lists, qcap each
   uint32_t *piv, *pivkey;  // pivot list, qcap each
   unsigned long long *slot;  // 3(n+1): partition-refinement pivot election, all ones between uses
-  uint32_t *aq;              // qcap: asynchronous reach queue, all ones (empty slots) between uses
+  uint32_t *aq;              // 2 qcap: asynchronous reach queue (bit 31: direction), all ones between uses
   uint32_t *hv, *hbeg, *hdeg, *htag, *hbase;  // heavy adjacency list split across the grid
   const uint32_t *seg;       // nseg+1 segment first ids (device) or null
   uint32_t *out_labels;      // optional destination of the final labels (device)

@@ -40,7 +40,7 @@ constexpr size_t a256(size_t x) { return (x + 255) & ~size_t(255); }
 constexpr uint32_t kWords = sccb::bitmap_words(kMaxN) + sccb::kBitmapSlack;
 constexpr size_t kVec = a256(size_t(kMaxN + 1) * 4);        // one u32 per vertex
 constexpr size_t kBitmaps = a256(size_t(kWords) * 4 * 7);   // elim, fvis, bvis, fexp, bexp, tflag, queued
-constexpr size_t kSlots = a256(size_t(kMaxN + 1) * (3 * 8 + 4));  // election slots + asynchronous reach queue
+constexpr size_t kSlots = a256(size_t(kMaxN + 1) * (3 * 8 + 8));  // election slots + asynchronous reach queue
 constexpr uint32_t kHeavyCap = kMaxM / 256u + 2u;
 constexpr size_t kHeavy = a256(size_t(kHeavyCap) * 5 * 4);
 constexpr size_t kCtl = a256(sizeof(sccb::Ctl));
@@ -181,7 +181,7 @@ extern "C" int scc_solve_noalloc(const scc_dev_csr *g, const scc_opts *opts, uin
 
   // the array keeps the previous call's contents: reset what must start fresh
   cudaError_t err = cudaMemsetAsync(s.ctl, 0, sizeof(sccb::Ctl), st);
-  if (err == cudaSuccess) err = cudaMemsetAsync(s.slot, 0xff, ((size_t)n + 1) * (3 * 8 + 4), st);
+  if (err == cudaSuccess) err = cudaMemsetAsync(s.slot, 0xff, ((size_t)n + 1) * (3 * 8 + 8), st);
   if (err != cudaSuccess) return sccb::set_error(SCC_ERR_CUDA, "scratch reset: %s", cudaGetErrorString(err));
   for (int t = 0; t < 2; ++t) {
     uint32_t bad = 0;
