@@ -38,6 +38,9 @@ constexpr uint32_t kLocalMax = 2048, kLocalEdges = 4096, kLocalLevels = 4096;
 constexpr uint32_t kWideDegree = 16;
 // polls of a partly filled window before an asynchronous step expands it
 constexpr uint32_t kAsyncHold = 1;
+// claims an asynchronous step keeps for the warp's next step (the rest go to
+// the shared queue)
+constexpr uint32_t kAsyncKeep = 32;
 // WCC switches from full sweeps to frontier sweeps once fewer than live / this
 // many colours change in a sweep
 constexpr uint32_t kWccFrontier = 64;
@@ -1468,17 +1471,35 @@ struct Eng {
   // and none can start.  Filled slots never wait long behind unfilled ones
   // of the same window (at most kAsyncHold polls).  Waits are bounded: no
   // progress for timeout_ns sets kErrBarrierTimeout.
-  // Appends the k claims staged in stb (all 32 lanes call) and counts
-  // `done` expanded sources, with one atomic on aq_td (tail << 32 | done).
-  __device__ __forceinline__ void async_append(const uint32_t *stb, uint32_t k, uint32_t done) {
+  // Ends (or, mid-step, drains) an asynchronous step: the k claims staged
+  // in stb are counted as created and `done` sources as expanded in one
+  // atomic on aq_td (created << 32 | expanded); at the end of a step
+  // (keep) up to kAsyncKeep - nl claims stay with this warp in loc for its
+  // next step, the rest are published to the queue.  Counting comes first,
+  // so an expansion is never counted before its vertex's creation (all 32
+  // lanes call).
+  __device__ __forceinline__ void async_commit(const uint32_t *stb, uint32_t k, uint32_t done, uint32_t *loc,
+                                               uint32_t &nl, bool keep) {
     __syncwarp();
-    unsigned long long old = 0;
-    if (lane_id() == 0 && (k | done)) old = atomicAdd(&c->aq_td, ((unsigned long long)k << 32) | done);
-    const uint32_t pos = (uint32_t)(__shfl_sync(kFull, old, 0) >> 32);
-    for (uint32_t i = lane_id(); i < k; i += 32u) {
-      if (pos + i < 2u * P.s.qcap) P.s.aq[pos + i] = stb[i];
-      else fail(kErrQueueOverflow);
+    const uint32_t lane = lane_id();
+    if (lane == 0 && (k | done)) atomicAdd(&c->aq_td, ((unsigned long long)k << 32) | done);
+    const uint32_t kept = keep ? (k < kAsyncKeep - nl ? k : kAsyncKeep - nl) : 0u;
+    for (uint32_t i = lane; i < kept; i += 32u) loc[nl + i] = stb[i];
+    const uint32_t npub = k - kept;
+    if (npub) {
+      uint32_t pos = 0;
+      if (lane == 0) {
+        __threadfence();  // the creation count is visible before any published item
+        pos = atomicAdd(&c->aq_pos, npub);
+      }
+      pos = __shfl_sync(kFull, pos, 0);
+      const uint32_t cap = 2u * P.s.qcap;
+      for (uint32_t i = lane; i < npub; i += 32u) {
+        if (pos + i < cap) P.s.aq[pos + i] = stb[kept + i];
+        else fail(kErrQueueOverflow);
+      }
     }
+    nl += kept;
     __syncwarp();
   }
 
@@ -1502,129 +1523,141 @@ struct Eng {
     const uint32_t qcap = 2u * s.qcap;
     if (is_lead()) {
       c->aq_head = 0;
+      c->aq_pos = ntot;
       c->aq_td = (unsigned long long)ntot << 32;
     }
     if (!bar(710)) return;
     const uint32_t lane = lane_id();
     uint32_t *const stb = stage_buf(0);  // this warp's claims of the current step
-    uint32_t steps = 0;  // warp steps (lane 0 counts them)
+    uint32_t *const loc = stage_buf(1);  // claims this warp keeps for its next step
+    uint32_t nl = 0;                     // kept claims (warp-uniform)
+    uint32_t steps = 0;                  // warp steps (lane 0 counts them)
     bool over = false;
+    uint32_t slot = 0;
+    bool pend = false;  // this lane's window slot is still to be expanded
+    unsigned long long idle0 = 0;
+    uint32_t nap = 32, idle = 0, hold = 0;
     while (!over) {
-      uint32_t base = 0;
-      if (lane == 0) base = atomicAdd(&c->aq_head, 32u);
-      base = __shfl_sync(kFull, base, 0);
-      if (base >= qcap) break;  // every slot is taken: nothing more can come this warp's way
-      const uint32_t slot = base + lane;
-      bool pend = slot < qcap;
-      unsigned long long idle0 = 0;
-      uint32_t nap = 32, idle = 0, hold = 0;
-      while (__any_sync(kFull, pend)) {
-        const uint32_t v = pend ? ldm(aq + slot) : kNone;
-        const bool rdy = pend && v != kNone;
-        const uint32_t rmask = __ballot_sync(kFull, rdy);
-        // a partly filled window is polled once more before it is
-        // expanded: while the reach is wide its other slots fill within
-        // nanoseconds, and a step then expands up to 32 vertices, not two
-        if (rmask && rmask != __ballot_sync(kFull, pend) && hold < kAsyncHold) {
-          ++hold;
-          __nanosleep(32);
-          continue;
+      if (!__any_sync(kFull, pend) && nl == 0) {
+        uint32_t base = 0;
+        if (lane == 0) base = atomicAdd(&c->aq_head, 32u);
+        base = __shfl_sync(kFull, base, 0);
+        if (base >= qcap) break;  // every slot is taken: nothing more can come this warp's way
+        slot = base + lane;
+        pend = slot < qcap;
+      }
+      const uint32_t wv = pend ? ldm(aq + slot) : kNone;
+      const bool rdy = pend && wv != kNone;
+      const uint32_t rmask = __ballot_sync(kFull, rdy);
+      // a partly filled window with nothing kept is polled once more before
+      // it is expanded: while the reach is wide its other slots fill within
+      // nanoseconds, and a step then expands up to 32 vertices, not two
+      if (nl == 0 && rmask && rmask != __ballot_sync(kFull, pend) && hold < kAsyncHold) {
+        ++hold;
+        __nanosleep(32);
+        continue;
+      }
+      // lanes without a filled slot take kept claims (from the top)
+      const uint32_t freem = ~rmask;
+      const uint32_t take = nl < (uint32_t)__popc(freem) ? nl : (uint32_t)__popc(freem);
+      const uint32_t rank = __popc(freem & lanemask_lt());
+      const bool fromloc = !rdy && rank < take;
+      const uint32_t v = rdy ? wv : fromloc ? loc[nl - 1u - rank] : kNone;
+      const bool have = rdy || fromloc;
+      const uint32_t hmask = __ballot_sync(kFull, have);
+      if (hmask) {
+        __syncwarp();  // kept claims read before the slots are reused below
+        nl -= take;
+        idle0 = 0;
+        nap = 32;
+        idle = 0;
+        hold = 0;
+        ++steps;
+        uint32_t b = 0, d = 0, rv = 0;
+        const uint32_t dir = have ? v >> 31 : 0u, x = v & 0x7fffffffu;
+        if (have) {
+          const uint32_t *off = dir ? g.offT : g.off;
+          b = ldg(off + x);
+          d = ldg(off + x + 1) - b;
+          rv = ranged ? ldm(s.range + x) : 0u;
         }
-        if (rmask) {
-          idle0 = 0;
-          nap = 32;
-          idle = 0;
-          hold = 0;
-          ++steps;
-          uint32_t b = 0, d = 0, rv = 0;
-          const uint32_t dir = rdy ? v >> 31 : 0u, x = v & 0x7fffffffu;
-          if (rdy) {
-            const uint32_t *off = dir ? g.offT : g.off;
-            b = ldg(off + x);
-            d = ldg(off + x + 1) - b;
-            rv = ranged ? ldm(s.range + x) : 0u;
-            aq[slot] = kNone;
+        if (rdy) aq[slot] = kNone;
+        pend = pend && !rdy;
+        // the 32 lists walked as one concatenation, four 32-edge rounds
+        // at a time with each round's loads issued together; claimed
+        // vertices wait in this warp's staging segment
+        const uint32_t incl = warp_incl_scan(d);
+        const uint32_t total = __shfl_sync(kFull, incl, 31);
+        const uint32_t excl = incl - d;
+        uint32_t nst = 0;  // staged claims (warp-uniform)
+        for (uint32_t e0 = 0; e0 < total; e0 += 128u) {
+          uint32_t u[4], rs[4], dr[4];
+          bool val[4];
+#pragma unroll
+          for (int r = 0; r < 4; ++r) {
+            const uint32_t e = e0 + 32u * r + lane;
+            uint32_t lo = 0;  // owner: largest lane whose slice starts at or before e
+#pragma unroll
+            for (uint32_t sft = 16; sft >= 1; sft >>= 1) {
+              const uint32_t cand = lo + sft;
+              const uint32_t ex = __shfl_sync(kFull, excl, cand & 31u);
+              if (cand < 32 && ex <= e) lo = cand;
+            }
+            const uint32_t o_beg = __shfl_sync(kFull, b, lo), o_ex = __shfl_sync(kFull, excl, lo);
+            rs[r] = __shfl_sync(kFull, rv, lo);
+            dr[r] = __shfl_sync(kFull, dir, lo);
+            val[r] = e < total;
+            u[r] = val[r] ? ldg((dr[r] ? g.adjT : g.adj) + o_beg + (e - o_ex)) : 0u;
           }
-          // the 32 lists walked as one concatenation, four 32-edge rounds
-          // at a time with each round's loads issued together; claimed
-          // vertices wait in this warp's staging segment
-          const uint32_t incl = warp_incl_scan(d);
-          const uint32_t total = __shfl_sync(kFull, incl, 31);
-          const uint32_t excl = incl - d;
-          uint32_t nst = 0;  // staged claims (warp-uniform)
-          for (uint32_t e0 = 0; e0 < total; e0 += 128u) {
-            uint32_t u[4], rs[4], dr[4];
-            bool val[4];
+          uint32_t vw[4], ew[4], rg[4];
 #pragma unroll
-            for (int r = 0; r < 4; ++r) {
-              const uint32_t e = e0 + 32u * r + lane;
-              uint32_t lo = 0;  // owner: largest lane whose slice starts at or before e
-#pragma unroll
-              for (uint32_t sft = 16; sft >= 1; sft >>= 1) {
-                const uint32_t cand = lo + sft;
-                const uint32_t ex = __shfl_sync(kFull, excl, cand & 31u);
-                if (cand < 32 && ex <= e) lo = cand;
-              }
-              const uint32_t o_beg = __shfl_sync(kFull, b, lo), o_ex = __shfl_sync(kFull, excl, lo);
-              rs[r] = __shfl_sync(kFull, rv, lo);
-              dr[r] = __shfl_sync(kFull, dir, lo);
-              val[r] = e < total;
-              u[r] = val[r] ? ldg((dr[r] ? g.adjT : g.adj) + o_beg + (e - o_ex)) : 0u;
-            }
-            uint32_t vw[4], ew[4], rg[4];
-#pragma unroll
-            for (int r = 0; r < 4; ++r) {
-              vw[r] = val[r] ? ldm((dr[r] ? s.bvis : s.fvis) + (u[r] >> 5)) : ~0u;
-              ew[r] = val[r] ? ldm(s.elim + (u[r] >> 5)) : ~0u;
-              rg[r] = val[r] && ranged ? ldm(s.range + u[r]) : rs[r];
-            }
-            bool cl[4];
-#pragma unroll
-            for (int r = 0; r < 4; ++r) {
-              const uint32_t bit = 1u << (u[r] & 31u);
-              cl[r] = !((vw[r] | ew[r]) & bit) && rg[r] == rs[r] &&
-                      !(atomicOr((dr[r] ? s.bvis : s.fvis) + (u[r] >> 5), bit) & bit);
-            }
-#pragma unroll
-            for (int r = 0; r < 4; ++r) {
-              const uint32_t m = __ballot_sync(kFull, cl[r]);
-              if (cl[r]) stb[nst + __popc(m & lanemask_lt())] = u[r] | (dr[r] << 31);
-              nst += __popc(m);
-            }
-            if (nst > kStage - 128u) {  // room for the next four rounds
-              async_append(stb, nst, 0u);
-              nst = 0;
-            }
+          for (int r = 0; r < 4; ++r) {
+            vw[r] = val[r] ? ldm((dr[r] ? s.bvis : s.fvis) + (u[r] >> 5)) : ~0u;
+            ew[r] = val[r] ? ldm(s.elim + (u[r] >> 5)) : ~0u;
+            rg[r] = val[r] && ranged ? ldm(s.range + u[r]) : rs[r];
           }
-          // one atomic reserves the staged claims' slots and counts this
-          // step's sources as expanded
-          async_append(stb, nst, (uint32_t)__popc(rmask));
-          pend = pend && !rdy;
-          continue;
-        }
-        // nothing filled: finished when every appended vertex is expanded.
-        // Checked on every eighth empty poll only: thousands of idle warps
-        // reading aq_td would queue ahead of the steps' atomics on it in its
-        // L2 slice.  Lane 0 decides for the warp, so the warp leaves as a
-        // whole.
-        uint32_t fin = 0;
-        if (lane == 0 && (++idle & 7u) == 0) {
-          const unsigned long long td = ld_acquire64(&c->aq_td);
-          fin = (uint32_t)(td >> 32) == (uint32_t)td || ldm(&c->gs.err) != 0;
-          if (!fin) {
-            const unsigned long long now = globaltimer_ns();
-            if (idle0 == 0) idle0 = now;
-            if (now - idle0 > P.o.timeout_ns) {
-              atomicOr(&c->gs.err, kErrBarrierTimeout);
-              atomicExch(&c->gs.err_where, 712u);
-              fin = 1;
-            }
+          bool cl[4];
+#pragma unroll
+          for (int r = 0; r < 4; ++r) {
+            const uint32_t bit = 1u << (u[r] & 31u);
+            cl[r] = !((vw[r] | ew[r]) & bit) && rg[r] == rs[r] &&
+                    !(atomicOr((dr[r] ? s.bvis : s.fvis) + (u[r] >> 5), bit) & bit);
+          }
+#pragma unroll
+          for (int r = 0; r < 4; ++r) {
+            const uint32_t m = __ballot_sync(kFull, cl[r]);
+            if (cl[r]) stb[nst + __popc(m & lanemask_lt())] = u[r] | (dr[r] << 31);
+            nst += __popc(m);
+          }
+          if (nst > kStage - 128u) {  // room for the next four rounds
+            async_commit(stb, nst, 0u, loc, nl, false);
+            nst = 0;
           }
         }
-        if (__shfl_sync(kFull, fin, 0)) {
-          over = true;
-          break;
+        async_commit(stb, nst, (uint32_t)__popc(hmask), loc, nl, true);
+        continue;
+      }
+      // nothing to expand: finished when every created vertex is expanded.
+      // Checked on every eighth empty poll only: thousands of idle warps
+      // reading aq_td would queue ahead of the steps' atomics on it in its
+      // L2 slice.  Lane 0 decides for the warp, so the warp leaves as a
+      // whole.
+      uint32_t fin = 0;
+      if (lane == 0 && (++idle & 7u) == 0) {
+        const unsigned long long td = ld_acquire64(&c->aq_td);
+        fin = (uint32_t)(td >> 32) == (uint32_t)td || ldm(&c->gs.err) != 0;
+        if (!fin) {
+          const unsigned long long now = globaltimer_ns();
+          if (idle0 == 0) idle0 = now;
+          if (now - idle0 > P.o.timeout_ns) {
+            atomicOr(&c->gs.err, kErrBarrierTimeout);
+            atomicExch(&c->gs.err_where, 712u);
+            fin = 1;
+          }
         }
+      }
+      if (__shfl_sync(kFull, fin, 0)) over = true;
+      else {
         __nanosleep(nap);
         if (nap < 256u) nap <<= 1;
       }

@@ -45,9 +45,10 @@ struct Ctl {
   uint32_t trace_n, trace_pad;
   uint32_t trace_slot[128], trace_a[128], trace_b[128];
   unsigned long long trace_ns[128];
-  // asynchronous reach: next slot to take; slots appended << 32 | vertices
-  // expanded (each in its own 128-byte line)
+  // asynchronous reach: next slot to take; next slot to fill; vertices
+  // created << 32 | vertices expanded (each in its own 128-byte line)
   uint32_t aq_head, aq_pad0[31];
+  uint32_t aq_pos, aq_pad2[31];
   unsigned long long aq_td, aq_pad1[15];
 };
 constexpr uint32_t kTrace = 128;
