@@ -1472,26 +1472,31 @@ struct Eng {
   // of the same window (at most kAsyncHold polls).  Waits are bounded: no
   // progress for timeout_ns sets kErrBarrierTimeout.
   // Ends (or, mid-step, drains) an asynchronous step: the k claims staged
-  // in stb are counted as created and `done` sources as expanded in one
-  // atomic on aq_td (created << 32 | expanded); at the end of a step
-  // (keep) up to kAsyncKeep - nl claims stay with this warp in loc for its
-  // next step, the rest are published to the queue.  Counting comes first,
-  // so an expansion is never counted before its vertex's creation (all 32
-  // lanes call).
+  // in stb are added to this warp's count of created vertices and `done` to
+  // its count of expanded ones; at the end of a step (keep) up to
+  // kAsyncKeep - nl claims stay with this warp in loc for its next step, and
+  // the rest are published to the queue.  The warp's counts reach aq_td
+  // (created << 32 | expanded) in one atomic before anything is published
+  // and whenever the warp runs out of work (async_flush), never otherwise:
+  // while a warp holds unflushed counts it has expanded vertices whose
+  // expansion the global count lacks, so the global counts cannot meet
+  // before that warp's work is done (all 32 lanes call).
   __device__ __forceinline__ void async_commit(const uint32_t *stb, uint32_t k, uint32_t done, uint32_t *loc,
-                                               uint32_t &nl, bool keep) {
+                                               uint32_t &nl, bool keep, unsigned long long &acc) {
     __syncwarp();
     const uint32_t lane = lane_id();
-    if (lane == 0 && (k | done)) atomicAdd(&c->aq_td, ((unsigned long long)k << 32) | done);
+    acc += ((unsigned long long)k << 32) | done;
     const uint32_t kept = keep ? (k < kAsyncKeep - nl ? k : kAsyncKeep - nl) : 0u;
     for (uint32_t i = lane; i < kept; i += 32u) loc[nl + i] = stb[i];
     const uint32_t npub = k - kept;
     if (npub) {
       uint32_t pos = 0;
       if (lane == 0) {
+        atomicAdd(&c->aq_td, acc);
         __threadfence();  // the creation count is visible before any published item
         pos = atomicAdd(&c->aq_pos, npub);
       }
+      acc = 0;
       pos = __shfl_sync(kFull, pos, 0);
       const uint32_t cap = 2u * P.s.qcap;
       for (uint32_t i = lane; i < npub; i += 32u) {
@@ -1501,6 +1506,10 @@ struct Eng {
     }
     nl += kept;
     __syncwarp();
+  }
+  __device__ __forceinline__ void async_flush(unsigned long long &acc) {
+    if (acc && lane_id() == 0) atomicAdd(&c->aq_td, acc);
+    acc = 0;
   }
 
   // Appends the frontier in[0, nin) of direction dir to the asynchronous
@@ -1531,6 +1540,7 @@ struct Eng {
     uint32_t *const stb = stage_buf(0);  // this warp's claims of the current step
     uint32_t *const loc = stage_buf(1);  // claims this warp keeps for its next step
     uint32_t nl = 0;                     // kept claims (warp-uniform)
+    unsigned long long acc = 0;          // this warp's unflushed counts (created << 32 | expanded)
     uint32_t steps = 0;                  // warp steps (lane 0 counts them)
     bool over = false;
     uint32_t slot = 0;
@@ -1542,7 +1552,10 @@ struct Eng {
         uint32_t base = 0;
         if (lane == 0) base = atomicAdd(&c->aq_head, 32u);
         base = __shfl_sync(kFull, base, 0);
-        if (base >= qcap) break;  // every slot is taken: nothing more can come this warp's way
+        if (base >= qcap) {  // every slot is taken: nothing more can come this warp's way
+          async_flush(acc);
+          break;
+        }
         slot = base + lane;
         pend = slot < qcap;
       }
@@ -1630,13 +1643,14 @@ struct Eng {
             nst += __popc(m);
           }
           if (nst > kStage - 128u) {  // room for the next four rounds
-            async_commit(stb, nst, 0u, loc, nl, false);
+            async_commit(stb, nst, 0u, loc, nl, false, acc);
             nst = 0;
           }
         }
-        async_commit(stb, nst, (uint32_t)__popc(hmask), loc, nl, true);
+        async_commit(stb, nst, (uint32_t)__popc(hmask), loc, nl, true, acc);
         continue;
       }
+      async_flush(acc);  // out of work: this warp's counts go out first
       // nothing to expand: finished when every created vertex is expanded.
       // Checked on every eighth empty poll only: thousands of idle warps
       // reading aq_td would queue ahead of the steps' atomics on it in its
