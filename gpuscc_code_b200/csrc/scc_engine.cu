@@ -64,9 +64,11 @@ struct Eng {
   // reach seeds and returns, and the caller runs both directions' phase
   uint32_t a_seeded;
   bool a_defer;
+  bool a_trim;  // trims run their worklist asynchronously (the solve, with async reaches on)
 
   __device__ explicit Eng(const Params &p)
-      : P(p), c(p.s.ctl), k(0), list_mode(0), act_count(0), act_sel(0), a_seeded(0), a_defer(false) {}
+      : P(p), c(p.s.ctl), k(0), list_mode(0), act_count(0), act_sel(0), a_seeded(0), a_defer(false),
+        a_trim(false) {}
 
   // ------------------------------------------------------------ plumbing
   __device__ __forceinline__ uint32_t *cur() { return c->ctr[k % 3]; }
@@ -421,6 +423,7 @@ struct Eng {
     const uint32_t lim = s.nwords * 32u;  // multiple of 1024
     const uint32_t lane = lane_id();
     const bool vec = ((reinterpret_cast<uintptr_t>(g.off) | reinterpret_cast<uintptr_t>(g.offT)) & 15u) == 0;
+    const bool vlab = (reinterpret_cast<uintptr_t>(s.label) & 15u) == 0;  // labels stored four at a time
     const uint32_t step = gstride() * 4u;
     struct Quad {
       uint32_t o[4], t[4], o4, t4;
@@ -510,7 +513,7 @@ struct Eng {
         const uint32_t din = (i < 3 ? q.t[i + 1] : t4) - q.t[i];
         if (v < 1u || v > n) continue;
         if (dout == 0 || din == 0) {
-          s.label[v] = v;
+          if (!vlab) s.label[v] = v;
           bits |= 1u << i;
           ++ntrim;
         } else if (dout == 1 || din == 1) {
@@ -519,6 +522,19 @@ struct Eng {
           const unsigned long long key = ((unsigned long long)prio(g, rule, v) << 32) | v;
           best = key < best ? key : best;
         }
+      }
+      if (vlab && v0 + 4u <= n + 1u) {
+        // one 16-byte store of the four labels: whole sectors written, no
+        // partial-sector merges in L2 (an id not trimmed here gets 0, and
+        // its label is written when it is eliminated; ambiguous ids are
+        // resolved below, after this store)
+        const uint4 l = make_uint4((bits & 1u) ? v0 : 0u, (bits & 2u) ? v0 + 1u : 0u, (bits & 4u) ? v0 + 2u : 0u,
+                                   (bits & 8u) ? v0 + 3u : 0u);
+        *reinterpret_cast<uint4 *>(s.label + v0) = l;
+      } else if (vlab) {
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+          if ((bits >> i) & 1u) s.label[v0 + i] = v0 + i;
       }
       // lanes 8j .. 8j+7 hold the 32 ids of word j of this warp's four
       const uint32_t grp = 0xffu << (lane & ~7u);
@@ -613,6 +629,14 @@ struct Eng {
     t0 = globaltimer_ns();
     uint32_t it = 1;
     uint32_t nq = rdprv(C_Q);
+    if (a_trim && nq > 0 && it < max_it) {
+      // the solve's range-aware trims: the worklist runs asynchronously
+      ntrim = async_trim(nq, ranged);
+      add_count(&c->n_trimmed, ntrim);
+      if (!bar(103)) return 2;
+      prof(PR_TRIM_WL, t0, 1);
+      return 2;
+    }
     while (nq > 0 && it < max_it) {
       // candidates: live partition-mates adjacent (either direction) to a vertex just trimmed
       for_items(nq, [&](uint32_t i, bool valid) {
@@ -1525,17 +1549,16 @@ struct Eng {
 
   // Expands the ntot items seeded in aq (bit 31: 0 = forward, 1 =
   // backward) and everything they reach, both directions at once.
-  __device__ __noinline__ void async_run(uint32_t ntot, bool ranged) {
+  // The loop of an asynchronous phase: windows of the shared queue, claims
+  // kept for the warp's next step, the warp's counts, termination (see
+  // async_run).  step(v, have, hmask, stb, loc, nl, acc) expands the lanes'
+  // items and ends with async_commit.  Returns this warp's step count
+  // (lane 0).
+  template <class Step>
+  __device__ __forceinline__ uint32_t async_loop(Step &&step) {
     const EngState &s = P.s;
-    const EngGraph &g = P.g;
     uint32_t *aq = s.aq;
     const uint32_t qcap = 2u * s.qcap;
-    if (is_lead()) {
-      c->aq_head = 0;
-      c->aq_pos = ntot;
-      c->aq_td = (unsigned long long)ntot << 32;
-    }
-    if (!bar(710)) return;
     const uint32_t lane = lane_id();
     uint32_t *const stb = stage_buf(0);  // this warp's claims of the current step
     uint32_t *const loc = stage_buf(1);  // claims this warp keeps for its next step
@@ -1586,6 +1609,52 @@ struct Eng {
         idle = 0;
         hold = 0;
         ++steps;
+        if (rdy) aq[slot] = kNone;  // consumed: the queue is all ones again after the phase
+        pend = pend && !rdy;
+        step(v, have, hmask, stb, loc, nl, acc);
+        continue;
+      }
+      async_flush(acc);  // out of work: this warp's counts go out first
+      // nothing to expand: finished when every created vertex is expanded.
+      // Checked on every eighth empty poll only: thousands of idle warps
+      // reading aq_td would queue ahead of the steps' atomics on it in its
+      // L2 slice.  Lane 0 decides for the warp, so the warp leaves as a
+      // whole.
+      uint32_t fin = 0;
+      if (lane == 0 && (++idle & 7u) == 0) {
+        const unsigned long long td = ld_acquire64(&c->aq_td);
+        fin = (uint32_t)(td >> 32) == (uint32_t)td || ldm(&c->gs.err) != 0;
+        if (!fin) {
+          const unsigned long long now = globaltimer_ns();
+          if (idle0 == 0) idle0 = now;
+          if (now - idle0 > P.o.timeout_ns) {
+            atomicOr(&c->gs.err, kErrBarrierTimeout);
+            atomicExch(&c->gs.err_where, 712u);
+            fin = 1;
+          }
+        }
+      }
+      if (__shfl_sync(kFull, fin, 0)) over = true;
+      else {
+        __nanosleep(nap);
+        if (nap < 256u) nap <<= 1;
+      }
+    }
+    return steps;
+  }
+
+  __device__ __noinline__ void async_run(uint32_t ntot, bool ranged) {
+    const EngState &s = P.s;
+    const EngGraph &g = P.g;
+    if (is_lead()) {
+      c->aq_head = 0;
+      c->aq_pos = ntot;
+      c->aq_td = (unsigned long long)ntot << 32;
+    }
+    if (!bar(710)) return;
+    const uint32_t lane = lane_id();
+    auto reach_step = [&](uint32_t v, bool have, uint32_t hmask, uint32_t *stb, uint32_t *loc, uint32_t &nl,
+                          unsigned long long &acc) {
         uint32_t b = 0, d = 0, rv = 0;
         const uint32_t dir = have ? v >> 31 : 0u, x = v & 0x7fffffffu;
         if (have) {
@@ -1594,8 +1663,6 @@ struct Eng {
           d = ldg(off + x + 1) - b;
           rv = ranged ? ldm(s.range + x) : 0u;
         }
-        if (rdy) aq[slot] = kNone;
-        pend = pend && !rdy;
         // the 32 lists walked as one concatenation, four 32-edge rounds
         // at a time with each round's loads issued together; claimed
         // vertices wait in this warp's staging segment
@@ -1648,37 +1715,89 @@ struct Eng {
           }
         }
         async_commit(stb, nst, (uint32_t)__popc(hmask), loc, nl, true, acc);
-        continue;
-      }
-      async_flush(acc);  // out of work: this warp's counts go out first
-      // nothing to expand: finished when every created vertex is expanded.
-      // Checked on every eighth empty poll only: thousands of idle warps
-      // reading aq_td would queue ahead of the steps' atomics on it in its
-      // L2 slice.  Lane 0 decides for the warp, so the warp leaves as a
-      // whole.
-      uint32_t fin = 0;
-      if (lane == 0 && (++idle & 7u) == 0) {
-        const unsigned long long td = ld_acquire64(&c->aq_td);
-        fin = (uint32_t)(td >> 32) == (uint32_t)td || ldm(&c->gs.err) != 0;
-        if (!fin) {
-          const unsigned long long now = globaltimer_ns();
-          if (idle0 == 0) idle0 = now;
-          if (now - idle0 > P.o.timeout_ns) {
-            atomicOr(&c->gs.err, kErrBarrierTimeout);
-            atomicExch(&c->gs.err_where, 712u);
-            fin = 1;
-          }
-        }
-      }
-      if (__shfl_sync(kFull, fin, 0)) over = true;
-      else {
-        __nanosleep(nap);
-        if (nap < 256u) nap <<= 1;
-      }
-    }
+    };
+    const uint32_t steps = async_loop(reach_step);
     add_count(cur() + C_CHG, lane == 0 ? steps : 0u);
     if (!bar(711)) return;
     if (is_lead()) c->phase_ret2 = rdprv(C_CHG);
+  }
+
+  // Asynchronous trim-1 worklist: the vertices trimmed by the sweep, in
+  // s.qa[0, nq), seed the queue; expanding a trimmed vertex t examines its
+  // live partition-mate neighbours (out- and in-lists) and trims each one
+  // left without a live partition-mate in- or out-neighbour, claiming it
+  // exactly once through its elim bit and appending it.  Same fixpoint as
+  // the synchronous iterations (a vertex's last relevant neighbour to go is
+  // expanded after its elim bit is set, and that expansion examines the
+  // vertex), without a grid barrier per iteration.  Returns the trimmed
+  // count of this thread.
+  __device__ __noinline__ uint32_t async_trim(uint32_t nq, bool ranged) {
+    const EngState &s = P.s;
+    const EngGraph &g = P.g;
+    async_seed(s.qa, nq, 0u, 0u);
+    if (is_lead()) {
+      c->aq_head = 0;
+      c->aq_pos = nq;
+      c->aq_td = (unsigned long long)nq << 32;
+    }
+    if (!bar(720)) return 0;
+    const uint32_t lane = lane_id();
+    uint32_t ntrim = 0;
+    auto trim_step = [&](uint32_t t, bool have, uint32_t hmask, uint32_t *stb, uint32_t *loc, uint32_t &nl,
+                         unsigned long long &acc) {
+      const uint32_t rt = have && ranged ? ldm(s.range + t) : 0u;
+      uint32_t nst = 0;
+      for (uint32_t pass = 0; pass < 2; ++pass) {  // out-lists, then in-lists
+        const uint32_t *off = pass ? g.offT : g.off, *adj = pass ? g.adjT : g.adj;
+        uint32_t b = 0, d = 0;
+        if (have) {
+          b = ldg(off + t);
+          d = ldg(off + t + 1) - b;
+        }
+        const uint32_t incl = warp_incl_scan(d);
+        const uint32_t total = __shfl_sync(kFull, incl, 31);
+        const uint32_t excl = incl - d;
+        for (uint32_t e0 = 0; e0 < total; e0 += 32u) {
+          const uint32_t e = e0 + lane;
+          uint32_t lo = 0;
+#pragma unroll
+          for (uint32_t sft = 16; sft >= 1; sft >>= 1) {
+            const uint32_t cand = lo + sft;
+            const uint32_t ex = __shfl_sync(kFull, excl, cand & 31u);
+            if (cand < 32 && ex <= e) lo = cand;
+          }
+          const uint32_t o_beg = __shfl_sync(kFull, b, lo), o_ex = __shfl_sync(kFull, excl, lo);
+          const uint32_t rs = __shfl_sync(kFull, rt, lo);
+          const bool val = e < total;
+          const uint32_t u = val ? ldg(adj + o_beg + (e - o_ex)) : 0u;
+          const uint32_t ew = val ? ldm(s.elim + (u >> 5)) : ~0u;
+          const uint32_t ru = val && ranged ? ldm(s.range + u) : rs;
+          const uint32_t bit = 1u << (u & 31u);
+          bool tr = false;
+          if (val && !(ew & bit) && ru == rs &&
+              !(live_nbr(s, g.off, g.adj, u, ru, ranged, false) && live_nbr(s, g.offT, g.adjT, u, ru, ranged, false))) {
+            tr = !(atomicOr(s.elim + (u >> 5), bit) & bit);
+            if (tr) {
+              atomicOr(s.tflag + (u >> 5), bit);
+              s.label[u] = u;
+              ++ntrim;
+            }
+          }
+          const uint32_t m = __ballot_sync(kFull, tr);
+          if (tr) stb[nst + __popc(m & lanemask_lt())] = u;
+          nst += __popc(m);
+          if (nst > kStage - 32u) {
+            async_commit(stb, nst, 0u, loc, nl, false, acc);
+            nst = 0;
+          }
+        }
+      }
+      async_commit(stb, nst, (uint32_t)__popc(hmask), loc, nl, true, acc);
+    };
+    const uint32_t steps = async_loop(trim_step);
+    (void)steps;
+    bar(721);
+    return ntrim;
   }
 
   // Worklist reach: DATA / LINEAR / TOPO / BEST.  Levels are synchronous:
@@ -2287,6 +2406,10 @@ struct Eng {
 
   __device__ void solve() {
     const EngOpts &o = P.o;
+    // asynchronous trim worklists on thin graphs, whose trims cascade over
+    // many iterations (elsewhere a trim's worklist is an iteration or two,
+    // cheaper than an asynchronous phase's seeding and barriers)
+    a_trim = o.async_depth >= 0 && (unsigned long long)P.g.m <= (unsigned long long)P.g.n * kAsyncTailDegree;
     const bool single = P.s.nseg <= 1;
     refresh_mode();
     unsigned long long t0 = globaltimer_ns();
