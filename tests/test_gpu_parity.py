@@ -77,6 +77,8 @@ def test_random_graphs_all_arms(ctx, alg):
     dict(alg="h", switch_permille=0, wcc=True, trim2=True),
     dict(alg="h", switch_permille=1000, wcc=True, trim2=True),
     dict(alg="t", grid_blocks=7),
+    dict(alg="h", wcc=True, trim2=True, async_depth=-1),
+    dict(alg="b", wcc=True, async_depth=1, block_size=1024),
 ])
 def test_option_space(ctx, opts):
     for name, g in random_graphs()[:4]:
