@@ -2771,6 +2771,13 @@ static cudaError_t coop_launch_occ(const Params &p, uint32_t phase, uint32_t a0,
 
 cudaError_t launch_phase(const Params &p, uint32_t phase, uint32_t a0, uint32_t a1, uint32_t a2, int block_size,
                          uint32_t grid_blocks, cudaStream_t stream, uint32_t *grid_used, int occupancy) {
+  // default register budget for 256-thread blocks: 80 registers (three CTAs
+  // per SM) on graphs of more than kAsyncTailDegree edges per vertex, whose
+  // solve is dominated by list sweeps that spill at 64; thin graphs keep
+  // four CTAs per SM (more warps for their latency-bound phases)
+  if (occupancy == 0 && block_size == 256 &&
+      (unsigned long long)p.g.m > (unsigned long long)p.g.n * kAsyncTailDegree)
+    occupancy = 3;
   switch (block_size) {
     case 128: return coop_launch_occ<128>(p, phase, a0, a1, a2, grid_blocks, stream, grid_used, occupancy);
     case 512: return coop_launch_occ<512>(p, phase, a0, a1, a2, grid_blocks, stream, grid_used, occupancy);

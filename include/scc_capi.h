@@ -85,7 +85,8 @@ typedef struct scc_opts {
   int32_t trim_first_depth;/* global trim-1 before the first pivot: 0 = to its fixpoint (reference trim1),
                               k > 0 = at most k iterations; later partition-aware trims remove the rest */
   int32_t occupancy;       /* register budget of the persistent kernel: 4 = four 256-thread CTAs per SM
-                              (64 registers), 3 = three (80 registers); 0 = engine default (4) */
+                              (64 registers), 3 = three (80 registers); 0 = engine default (256-thread
+                              blocks: 3 on graphs of more than 12 edges per vertex, else 4) */
   int32_t async_depth;     /* TOPO / BEST / HYBRID reaches: after this many synchronous levels, a frontier of
                               at most 8 edges per vertex is expanded asynchronously (every warp takes queued
                               vertices as they are appended, no level barriers; for deep, thin reaches such as
