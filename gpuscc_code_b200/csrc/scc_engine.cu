@@ -1482,19 +1482,22 @@ struct Eng {
   // frontier is copied into the queue aq (async_seed; in the solve the
   // forward and the backward reach both seed it, items tagged with their
   // direction in bit 31, and their asynchronous parts run as one phase, so
-  // a round costs the deeper of the two reaches, not their sum); every
-  // warp repeatedly takes the next 32 slots (one atomicAdd on aq_head),
-  // expands the vertices of its slots as they are filled (the 32 lists
-  // walked as one concatenation, 128 edges per round of loads), and appends
-  // every vertex it claims (exactly once, through the visited bitmap) with
-  // one atomic per step on aq_td, which holds the slots appended (high
-  // half) and the vertices expanded (low half).  A consumed slot is reset to
-  // kNone, so aq is all ones again when the reach ends.  The reach is over
-  // when the two halves are equal: a step's appends are counted in the same
-  // atomic as its sources, so equal halves mean no expansion is in flight
-  // and none can start.  Filled slots never wait long behind unfilled ones
-  // of the same window (at most kAsyncHold polls).  Waits are bounded: no
-  // progress for timeout_ns sets kErrBarrierTimeout.
+  // a round costs the deeper of the two reaches, not their sum).  Every
+  // warp takes the next 32 slots (one atomicAdd on aq_head) whenever it has
+  // nothing else to do, expands the vertices of its slots as they are
+  // filled (the 32 lists walked as one concatenation, 128 edges per round
+  // of loads) and claims new vertices exactly once through the visited
+  // bitmap.  Up to kAsyncKeep of a step's claims stay with the warp for its
+  // next step; the rest are published at aq_pos.  aq_td holds the vertices
+  // created (high half: seeds and claims) and expanded (low half); a warp
+  // adds its counts to it before it publishes and when it runs out of
+  // work, so the halves can only meet when no expansion is in flight and
+  // none can start, which ends the phase.  A consumed slot is reset to
+  // kNone, so aq is all ones again when the phase ends.  Filled slots never
+  // wait long behind unfilled ones of the same window (at most kAsyncHold
+  // polls).  Waits are bounded: no progress for timeout_ns sets
+  // kErrBarrierTimeout.  async_loop holds this machinery; async_run and
+  // async_trim supply the expansion step.
   // Ends (or, mid-step, drains) an asynchronous step: the k claims staged
   // in stb are added to this warp's count of created vertices and `done` to
   // its count of expanded ones; at the end of a step (keep) up to
