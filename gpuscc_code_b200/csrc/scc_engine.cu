@@ -38,6 +38,9 @@ constexpr uint32_t kLocalMax = 2048, kLocalEdges = 4096, kLocalLevels = 4096;
 constexpr uint32_t kWideDegree = 16;
 // polls of a partly filled window before an asynchronous step expands it
 constexpr uint32_t kAsyncHold = 1;
+// frontiers below this many vertices stay in CTA-local levels rather than
+// starting an asynchronous phase
+constexpr uint32_t kAsyncMin = 32;
 // claims an asynchronous step keeps for the warp's next step (the rest go to
 // the shared queue)
 constexpr uint32_t kAsyncKeep = 32;
@@ -1166,7 +1169,8 @@ struct Eng {
   // Results for the level driver go to cur()[C_L*]; C_LREF = 1 when the
   // frontier's edges exceed kLocalEdges (nothing done).
   __device__ __noinline__ void local_levels(const uint32_t *__restrict__ off, const uint32_t *__restrict__ adj, uint32_t *vis,
-                               bool ranged, const uint32_t *in, uint32_t nin, uint32_t sel, uint32_t max_levels) {
+                               bool ranged, const uint32_t *in, uint32_t nin, uint32_t sel, uint32_t max_levels,
+                               uint32_t stop_at) {
     const EngState &s = P.s;
     __shared__ uint32_t s_cnt, s_deg;
     // source table of the current chunk, in the staging segments (no stage
@@ -1268,7 +1272,7 @@ struct Eng {
       lin = lout;
       lsel ^= 1u;
       __syncthreads();
-      if (lnin > kLocalMax || lmf > kLocalEdges) break;
+      if (lnin > kLocalMax || lmf > kLocalEdges || lnin >= stop_at) break;
     }
     if (threadIdx.x == 0) {
       uint32_t *o = cur();
@@ -1837,9 +1841,15 @@ struct Eng {
     // thin, deep reaches continue asynchronously (the frontier's edges are
     // known only where pulls are allowed)
     const uint32_t async_after = async_from != kNone ? async_from : P.o.async_depth > 0 ? (uint32_t)P.o.async_depth : kNone;
+    const bool thin = (unsigned long long)P.g.m <= (unsigned long long)P.g.n * kAsyncTailDegree;
     while (nin > 0 || partial) {
       const unsigned long long ts = globaltimer_ns();
-      if (allow_pull && !pull && !partial && depth >= async_after && mf <= (unsigned long long)nin * 8ull) {
+      // (on graphs that are not thin, a frontier of a few vertices -- the
+      // end of a power-law reach -- finishes or grows in CTA-local levels
+      // first: an asynchronous phase's seeding and barriers cost more; thin
+      // graphs' deep reaches go asynchronous at once)
+      const bool may_async = allow_pull && !pull && !partial && depth >= async_after;
+      if (may_async && (nin >= kAsyncMin || thin) && mf <= (unsigned long long)nin * 8ull) {
         // the frontier goes to the asynchronous queue; with a_defer the
         // other direction's reach runs first and both finish together
         async_seed(in, nin, a_seeded, dir);
@@ -1855,7 +1865,8 @@ struct Eng {
         uint32_t lroom = room < kLocalLevels ? room : kLocalLevels;
         // a reach that may turn asynchronous stops its local levels there
         if (allow_pull && depth < async_after && async_after - depth < lroom) lroom = async_after - depth;
-        if (blockIdx.x == 0) local_levels(off, adj, vis, ranged, in, nin, sel, lroom);
+        if (blockIdx.x == 0)
+          local_levels(off, adj, vis, ranged, in, nin, sel, lroom, may_async && !thin ? kAsyncMin : kNone);
         if (!bar(704)) return depth;
         if (!rdprv(C_LREF) && rdprv(C_LD) > 0) {
           const uint32_t ld = rdprv(C_LD);
